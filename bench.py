@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Throughput of the advection hot path on the B200, one JSON line.
+
+Workload (the throughput configuration): a 256^3 FP32 curl-noise field
+(sigma 4 cells, field seed 1, spacing 1, unit RMS speed), 1,048,576 seeds
+uniform in the valid domain [0, 255)^3 (seed 1; rank r uses seed 1 + r),
+runge_kutta_4 with the reference's semantics, step 0.25, 2000 iterations,
+end positions only. One bench step advects every seed through all its
+iterations: particle state reset on the device, processing order, advection.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+`value` is whole-job particle-steps/s (steps actually taken, summed over
+ranks, divided by the max over ranks of the device-timed step). `e2e` is the
+same metric through the host C ABI call (dpa_advect_round) with pinned host
+buffers, copies included. The CPU baseline is the oracle's reference-faithful
+restatement on a bounded seed sample on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "RK4 particle-steps/s vs plain FP32 GPU & host TBB; served p50/p99 latency"
+UNIT = "particle-steps/s"
+FALLBACK_HBM_GBS = 6650.0
+BYTES_PER_STEP = {"f32": 96, "f16": 48, "bf16": 48}  # 8 corners x 3 components
+STATE_BYTES = 12 + 8 + 12 + 8 + 1  # positions + remaining in, out + termination
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="dpa_b200", choices=["dpa_b200", "reference"])
+    p.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
+    p.add_argument("--integrator", default="runge_kutta_4")
+    p.add_argument("--n", type=int, default=256)
+    p.add_argument("--seeds", type=int, default=1 << 20)
+    p.add_argument("--iterations", type=int, default=2000)
+    p.add_argument("--step-size", type=float, default=0.25)
+    p.add_argument("--cpu-seconds", type=float, default=10.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def workload_config(a, world):
+    return {
+        "workload": f"curl-noise {a.n}^3 {a.storage.upper()} field (sigma 4, seed 1, spacing 1), "
+                    f"{a.seeds} uniform seeds per rank (seed 1+rank) in [0,{a.n - 1})^3, "
+                    f"{a.integrator} (one field sample per step), step {a.step_size}, "
+                    f"{a.iterations} iterations, end positions only",
+        "field_shape": [a.n, a.n, a.n],
+        "seeds_per_rank": a.seeds,
+        "iterations": a.iterations,
+        "step_size": a.step_size,
+        "integrator": a.integrator,
+        "storage": a.storage,
+        "parallelism": f"replicas x{world} (independent seed sets, no collective)",
+        "l2": "256 MiB buffer written between timed steps (L2 flush)",
+    }
+
+
+def measured_peak_hbm():
+    path = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(path.read_text())
+        return float(d["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback 6.65 TB/s (MEASURED_PEAKS.json absent)"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            threading.Thread(target=self._read, daemon=True).start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        sms, maxes, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sms.append(float(parts[1]))
+                maxes.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sms:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sms), "sm_max_mhz": max(maxes),
+                "reasons": sorted(reasons), "samples": len(sms)}
+
+
+def make_inputs(a, rank, device):
+    from dpa_b200 import fields, seeds
+    grid = fields.curl_noise(a.n, 4.0, 1, spacing=1.0, device=device)
+    offset, size = seeds.seed_box(grid)
+    box = ([0.0, 0.0, 0.0], [float(a.n - 1)] * 3)
+    parts = seeds.generate_random(offset, size, a.seeds, a.iterations, aabb=box, seed=1 + rank)
+    return grid, parts
+
+
+def cpu_baseline(a, grid, parts, target_seconds, steps_budget=None):
+    """The oracle's reference-faithful restatement on a seed sample sized for
+    about `target_seconds` of work on all host threads."""
+    from oracle import binding as ob
+    ob.build()
+    threads = os.cpu_count() or 1
+    ob.set_threads(threads)
+    og = ob.OracleGrid.of(grid)
+    rem = np.full(a.seeds, a.iterations, np.uint64)
+    calib = max(threads * 8, 64)
+    t0 = time.perf_counter()
+    r = ob.advect_round(og, a.integrator, a.step_size, parts.position[:calib], rem[:calib])
+    dt = time.perf_counter() - t0
+    rate = float(np.sum(r.steps)) / max(dt, 1e-9)
+    steps_per_particle = max(float(np.mean(r.steps)), 1.0)
+    count = int(min(a.seeds, max(calib, rate * target_seconds / steps_per_particle)))
+    t0 = time.perf_counter()
+    r = ob.advect_round(og, a.integrator, a.step_size, parts.position[:count], rem[:count])
+    dt = time.perf_counter() - t0
+    taken = float(np.sum(r.steps))
+    return {"value": taken / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"first {count} of the {a.seeds} seeds at full {a.iterations} iterations "
+                      f"({int(taken)} particle-steps in {dt:.2f} s; oracle/oracle.cpp, "
+                      "OpenMP dynamic schedule standing in for TBB)"}
+
+
+def fp64_error(a, grid, gpu_positions, parts, sample=256):
+    """Position error of the GPU result against the FP64 oracle integrator,
+    in cells, over the first `sample` seeds that complete in both."""
+    from oracle import binding as ob
+    ob.build()
+    ob.set_threads(os.cpu_count() or 1)
+    og = ob.OracleGrid.of(grid)
+    rem = np.full(sample, a.iterations, np.uint64)
+    r = ob.advect64(og, a.integrator, a.step_size, parts.position[:sample], rem)
+    ok = r.termination == 0
+    err = np.linalg.norm(gpu_positions[:sample][ok].astype(np.float64) - r.positions[ok], axis=1)
+    err = err / float(grid.spacing[0])
+    return {"sample": sample, "completed": int(ok.sum()),
+            "median_cells": float(np.median(err)) if ok.any() else None,
+            "p90_cells": float(np.percentile(err, 90)) if ok.any() else None,
+            "note": "chaotic random field: FP32 rounding differences grow along trajectories"}
+
+
+def run_reference(a):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return 0
+    device = "cuda" if _cuda_available() else None
+    grid, parts = make_inputs(a, 0, device)
+    per_step = max(2.0, min(8.0, 150.0 / max(a.steps + a.warmup, 1)))
+    for _ in range(a.warmup):
+        cpu_baseline(a, grid, parts, per_step / 4)
+    values, samples = [], []
+    for _ in range(a.steps):
+        b = cpu_baseline(a, grid, parts, per_step)
+        values.append(b["value"])
+        samples.append(b["sample"])
+    value = statistics.mean(values)
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": None, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(a, 1),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                         "sample": samples[-1]},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference cannot be built here (Boost, Eigen, TBB, HDF5, MPI absent); this "
+                "arm times oracle/oracle.cpp, its reference-faithful C++ restatement",
+    }
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+def _cuda_available():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def run_gpu(a):
+    import ctypes as C
+    import torch
+    import torch.distributed as dist
+    import dpa_b200
+    from dpa_b200 import _native as N
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    grid, parts = make_inputs(a, rank, "cuda")
+    ctx = dpa_b200.Context(local)
+    lib = ctx._lib
+    field = ctx.field(grid, a.storage)
+    n = a.seeds
+    pristine_pos = torch.from_numpy(parts.position).cuda()
+    pristine_rem = torch.full((n,), a.iterations, dtype=torch.int64, device="cuda")
+    pos = torch.empty_like(pristine_pos)
+    rem = torch.empty_like(pristine_rem)
+    term = torch.empty(n, dtype=torch.uint8, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    opts = N.AdvectOptions(N.INTEGRATORS[a.integrator], float(np.float32(a.step_size)), 0, 0, 0, 1)
+    stream = torch.cuda.current_stream()
+    ctx.check(lib.dpa_context_set_profiling(ctx.handle, 1))
+
+    def one_step():
+        pos.copy_(pristine_pos)
+        rem.copy_(pristine_rem)
+        ctx.check(lib.dpa_advect_device(ctx.handle, field.handle, C.byref(opts), n,
+                                        C.c_void_p(pos.data_ptr()), C.c_void_p(rem.data_ptr()),
+                                        C.c_void_p(term.data_ptr()), C.c_void_p(stream.cuda_stream)))
+
+    for _ in range(a.warmup):
+        flush.fill_(1)
+        one_step()
+    torch.cuda.synchronize()
+
+    launches0 = C.c_uint64()
+    ctx.check(lib.dpa_context_launch_count(ctx.handle, C.byref(launches0)))
+    clocks = ClockSampler(local)
+    clocks.start()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    total_ms, kernel_ms, order_ms = 0.0, [], []
+    for _ in range(a.steps):
+        flush.fill_(2)
+        start = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        one_step()
+        end.record(stream)
+        end.synchronize()
+        total_ms += start.elapsed_time(end)
+        o, k = C.c_float(), C.c_float()
+        ctx.check(lib.dpa_context_last_timing(ctx.handle, C.byref(o), C.byref(k)))
+        order_ms.append(o.value)
+        kernel_ms.append(k.value)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clock_info = clocks.stop()
+    launches1 = C.c_uint64()
+    ctx.check(lib.dpa_context_launch_count(ctx.handle, C.byref(launches1)))
+    gpu_launches = int(launches1.value - launches0.value)
+
+    rem_out = rem.cpu().numpy().astype(np.int64)
+    steps_taken = float(np.sum(a.iterations - rem_out))
+    ms_per_step = total_ms / a.steps
+    t = torch.tensor([ms_per_step], dtype=torch.float64, device="cuda")
+    s = torch.tensor([steps_taken], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(s, op=dist.ReduceOp.SUM)
+    ms_max = float(t.item())
+    value = float(s.item()) / (ms_max / 1e3)
+    gpu_final = pos.cpu().numpy()
+
+    # End to end through the host C ABI with pinned host buffers.
+    host_pos = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+    host_rem = torch.empty(n, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+    host_term = torch.empty(n, dtype=torch.uint8, pin_memory=True).numpy()
+    e2e_steps = max(1, min(a.steps, 3))
+    e2e_opts = N.AdvectOptions(N.INTEGRATORS[a.integrator], float(np.float32(a.step_size)), 0, 0, 0, 1)
+
+    def e2e_once():
+        host_pos[:] = parts.position
+        host_rem[:] = a.iterations
+        t0 = time.perf_counter()
+        ctx.check(lib.dpa_advect_round(ctx.handle, field.handle, C.byref(e2e_opts), n,
+                                       host_pos.ctypes.data_as(C.c_void_p),
+                                       host_rem.ctypes.data_as(C.c_void_p),
+                                       host_term.ctypes.data_as(C.c_void_p), N.CURVE_SINK(), None))
+        return time.perf_counter() - t0
+
+    e2e_once()
+    e2e_times = [e2e_once() for _ in range(e2e_steps)]
+    e2e_steps_taken = float(np.sum(a.iterations - host_rem.astype(np.int64)))
+    e2e_t = torch.tensor([statistics.mean(e2e_times)], dtype=torch.float64, device="cuda")
+    e2e_s = torch.tensor([e2e_steps_taken], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(e2e_s, op=dist.ReduceOp.SUM)
+    e2e_value = float(e2e_s.item()) / float(e2e_t.item())
+
+    peak, peak_src = measured_peak_hbm()
+    kernel_s = statistics.mean(kernel_ms) / 1e3
+    algorithmic = BYTES_PER_STEP[a.storage] * steps_taken + STATE_BYTES * n
+    achieved = algorithmic / kernel_s / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "advect_traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get(f"{a.storage}_{a.integrator}_n{a.n}")
+        except Exception:
+            traffic = None
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(a, world),
+        "particle_steps_per_step": float(s.item()),
+        "kernel_ms": statistics.mean(kernel_ms), "order_ms": statistics.mean(order_ms),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic,
+                     "peak_source": peak_src,
+                     "algorithmic_bytes": f"{BYTES_PER_STEP[a.storage]} B per particle-step "
+                                          f"(8 corners x 3 x {BYTES_PER_STEP[a.storage] // 24} B)"
+                                          f" + {STATE_BYTES} B particle state per particle",
+                     "kernel": "advect_kernel (CUDA events around its launch, on its stream)"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n * (12 + 8),
+                "d2h_bytes_per_step": n * (12 + 8 + 1),
+                "call": "dpa_advect_round with pinned host buffers (wall clock around the "
+                        "synchronous call)"},
+        "gpu_launches": gpu_launches,
+        "clocks": clock_info,
+    }
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(a, grid, parts, a.cpu_seconds)
+        out["fp64_error"] = fp64_error(a, grid, gpu_final, parts)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    field.close()
+    ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    a = parse_args()
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_gpu(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

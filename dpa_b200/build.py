@@ -1,0 +1,93 @@
+"""Build recipe of the native parts: the sm_100a CUDA library and the C++ host
+pipeline.
+
+    python -m dpa_b200.build            # builds everything in-tree
+
+Outputs (git-ignored, shipped with the tree):
+    dpa_b200/libdpa_b200.so     C ABI of include/dpa_b200.h (CUDA, sm_100a)
+    dpa_b200/bin/dpa_pipeline   drop-in for the reference's `dpa config.json`
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PACKAGE = Path(__file__).resolve().parent
+ROOT = PACKAGE.parent
+CSRC = PACKAGE / "csrc"
+HOST = PACKAGE / "host"
+INCLUDE = ROOT / "include"
+LIBRARY = PACKAGE / "libdpa_b200.so"
+PIPELINE = PACKAGE / "bin" / "dpa_pipeline"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+CUDA_SOURCES = ["capi.cu", "advect.cu", "emit.cu", "ftle.cu"]
+
+
+def nvcc() -> str:
+    for candidate in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if candidate and Path(candidate).exists():
+            return candidate
+    raise RuntimeError("nvcc not found")
+
+
+def _stale(target: Path, sources: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(s.stat().st_mtime > t for s in sources)
+
+
+def _run(cmd: list[str]) -> None:
+    print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+
+
+def build_library(force: bool = False, verbose_ptxas: bool = False) -> Path:
+    sources = [CSRC / s for s in CUDA_SOURCES]
+    deps = sources + list(CSRC.glob("*.cuh")) + [INCLUDE / "dpa_b200.h"]
+    if not force and not _stale(LIBRARY, deps):
+        return LIBRARY
+    build_dir = PACKAGE / "_build"
+    build_dir.mkdir(exist_ok=True)
+    objects = []
+    flags = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
+                    "-I", str(INCLUDE), "-I", str(CSRC), "--expt-relaxed-constexpr"]
+    if verbose_ptxas:
+        flags += ["-Xptxas", "-v"]
+    for src in sources:
+        obj = build_dir / (src.stem + ".o")
+        _run([nvcc(), "-c", str(src), "-o", str(obj)] + flags)
+        objects.append(str(obj))
+    tmp = LIBRARY.with_suffix(".so.tmp")
+    _run([nvcc()] + ARCH + ["-shared", "-o", str(tmp)] + objects + ["-cudart", "static"])
+    os.replace(tmp, LIBRARY)
+    return LIBRARY
+
+
+def build_pipeline(force: bool = False) -> Path | None:
+    sources = sorted(HOST.glob("*.cpp"))
+    if not sources:
+        return None
+    deps = sources + sorted(HOST.glob("*.hpp")) + [INCLUDE / "dpa_b200.h", LIBRARY]
+    if not force and not _stale(PIPELINE, deps):
+        return PIPELINE
+    PIPELINE.parent.mkdir(exist_ok=True)
+    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", str(INCLUDE), "-I", str(HOST)]
+    cmd += [str(s) for s in sources]
+    cmd += ["-o", str(PIPELINE), "-L", str(PACKAGE), "-ldpa_b200",
+            "-Wl,-rpath,$ORIGIN/..", "-lpthread"]
+    _run(cmd)
+    return PIPELINE
+
+
+def build(force: bool = False) -> None:
+    build_library(force=force)
+    build_pipeline(force=force)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv)

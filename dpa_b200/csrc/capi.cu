@@ -1,0 +1,821 @@
+// capi.cu -- the C ABI of include/dpa_b200.h: contexts, fields, rounds, FTLE.
+//
+// Host orchestration only; the kernels live in advect.cu, emit.cu and ftle.cu.
+// Every entry point returns a dpa_status, records a message on failure and
+// never lets a C++ exception cross the boundary.
+#include <cub/device/device_scan.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace {
+
+struct DeviceBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  cudaError_t reserve(size_t n) {
+    if (n <= bytes && ptr) return cudaSuccess;
+    release();
+    if (n == 0) n = 16;
+    cudaError_t e = cudaMalloc(&ptr, n);
+    if (e != cudaSuccess) {
+      ptr = nullptr;
+      return e;
+    }
+    bytes = n;
+    return cudaSuccess;
+  }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(ptr); }
+};
+
+struct PinnedBuffer {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  cudaError_t reserve(size_t n) {
+    if (n <= bytes && ptr) return cudaSuccess;
+    release();
+    if (n == 0) n = 16;
+    cudaError_t e = cudaMallocHost(&ptr, n);
+    if (e != cudaSuccess) {
+      ptr = nullptr;
+      return e;
+    }
+    bytes = n;
+    return cudaSuccess;
+  }
+  void release() {
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  template <class T>
+  T* as() const { return static_cast<T*>(ptr); }
+};
+
+}  // namespace
+
+struct dpa_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string error;
+  uint64_t staging_limit = 1ull << 30;
+
+  DeviceBuffer positions, remaining, remaining_in, termination;
+  DeviceBuffer keys, values, sort_temp;
+  uint64_t launches = 0;  // kernels this context launched (advection path)
+  bool profiling = false;
+  cudaEvent_t events[3] = {nullptr, nullptr, nullptr};  // order, advect begin, advect end
+  bool timed_order = false;
+  DeviceBuffer raw, raw_offsets, raw_counts, kept_vertices, kept_segments;
+  DeviceBuffer wide, vertex_offsets, segment_offsets, scan_temp, totals;
+  DeviceBuffer out_vertices, out_colors, out_indices;
+  PinnedBuffer host_vertices, host_colors, host_indices, host_totals;
+  DeviceBuffer ftle_winners, ftle_flow, ftle_out, ftle_original, ftle_final;
+
+  void release_all() {
+    DeviceBuffer* d[] = {&positions, &remaining, &remaining_in, &termination, &keys, &values,
+                         &sort_temp, &raw, &raw_offsets, &raw_counts,
+                         &kept_vertices, &kept_segments, &wide, &vertex_offsets,
+                         &segment_offsets, &scan_temp, &totals, &out_vertices, &out_colors,
+                         &out_indices, &ftle_winners, &ftle_flow, &ftle_out, &ftle_original,
+                         &ftle_final};
+    for (DeviceBuffer* b : d) b->release();
+    PinnedBuffer* h[] = {&host_vertices, &host_colors, &host_indices, &host_totals};
+    for (PinnedBuffer* b : h) b->release();
+  }
+};
+
+struct dpa_field {
+  dpa_context* owner = nullptr;
+  DeviceBuffer nodes;
+  dpa::FieldView view{};
+  uint64_t shape[3] = {0, 0, 0};
+  float offset[3] = {0, 0, 0};
+  float spacing[3] = {0, 0, 0};
+  int32_t storage = DPA_STORAGE_F32;
+};
+
+namespace {
+
+int fail(dpa_context* ctx, int status, const std::string& message) {
+  if (ctx) ctx->error = message;
+  return status;
+}
+
+int fail_cuda(dpa_context* ctx, cudaError_t e, const char* where) {
+  const int status = (e == cudaErrorMemoryAllocation) ? DPA_ERROR_OUT_OF_MEMORY : DPA_ERROR_CUDA;
+  return fail(ctx, status, std::string(where) + ": " + cudaGetErrorName(e) + " (" +
+                               cudaGetErrorString(e) + ")");
+}
+
+#define DPA_TRY_CUDA(ctx, expr)                                  \
+  do {                                                           \
+    cudaError_t dpa_e_ = (expr);                                 \
+    if (dpa_e_ != cudaSuccess) return fail_cuda(ctx, dpa_e_, #expr); \
+  } while (0)
+
+template <class F>
+int guarded(dpa_context* ctx, F&& body) {
+  try {
+    return body();
+  } catch (const std::bad_alloc&) {
+    return fail(ctx, DPA_ERROR_OUT_OF_MEMORY, "host allocation failed");
+  } catch (const std::exception& e) {
+    return fail(ctx, DPA_ERROR_INTERNAL, e.what());
+  } catch (...) {
+    return fail(ctx, DPA_ERROR_INTERNAL, "unknown exception");
+  }
+}
+
+bool is_power_of_two(float h) {
+  if (!(h > 0.0f) || !std::isfinite(h)) return false;
+  int e = 0;
+  return std::frexp(h, &e) == 0.5f && std::ldexp(1.0f, e - 1) == h &&
+         std::isnormal(1.0f / h);
+}
+
+cudaStream_t pick_stream(dpa_context* ctx, void* stream) {
+  return stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+}
+
+int check_options(dpa_context* ctx, const dpa_advect_options* o) {
+  if (!o) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "options is NULL");
+  switch (o->integrator) {
+    case DPA_INTEGRATOR_EULER:
+    case DPA_INTEGRATOR_RUNGE_KUTTA_4:
+    case DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE:
+      break;
+    case DPA_INTEGRATOR_MODIFIED_MIDPOINT:
+    case DPA_INTEGRATOR_RUNGE_KUTTA_CASH_KARP_54:
+    case DPA_INTEGRATOR_RUNGE_KUTTA_DORMAND_PRINCE_5:
+    case DPA_INTEGRATOR_RUNGE_KUTTA_FEHLBERG_78:
+    case DPA_INTEGRATOR_ADAMS_BASHFORTH_2:
+    case DPA_INTEGRATOR_ADAMS_BASHFORTH_MOULTON_2:
+      return fail(ctx, DPA_ERROR_UNSUPPORTED,
+                  "integrator " + std::to_string(o->integrator) +
+                      " is not implemented on the GPU (euler, runge_kutta_4 and "
+                      "runge_kutta_4_true are)");
+    default:
+      return fail(ctx, DPA_ERROR_INVALID_ARGUMENT,
+                  "unknown integrator " + std::to_string(o->integrator));
+  }
+  if (!std::isfinite(o->step_size))
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "step_size is not finite");
+  return DPA_OK;
+}
+
+// Builds the processing order of `count` device positions (coarse Morton
+// buckets, see launch_order) in ctx->values. Returns it through *order.
+int build_order(dpa_context* ctx, const dpa_field* field, const float* positions, uint64_t count,
+                cudaStream_t stream, const uint32_t** order) {
+  *order = nullptr;
+  if (count < 2) return DPA_OK;
+  DPA_TRY_CUDA(ctx, ctx->keys.reserve(count * 2));
+  DPA_TRY_CUDA(ctx, ctx->values.reserve(count * 4));
+  DPA_TRY_CUDA(ctx, ctx->sort_temp.reserve((dpa::kOrderBuckets + 1) * 4));
+  DPA_TRY_CUDA(ctx, dpa::launch_order(field->view, positions, count, ctx->keys.as<uint16_t>(),
+                                      ctx->sort_temp.as<uint32_t>(), ctx->values.as<uint32_t>(),
+                                      stream));
+  ctx->launches += dpa::kOrderLaunches;
+  *order = ctx->values.as<uint32_t>();
+  return DPA_OK;
+}
+
+// Order (optional) + advection kernel over device arrays, no recording.
+int advect_device_impl(dpa_context* ctx, const dpa_field* field, const dpa_advect_options* o,
+                       uint64_t count, float* positions, uint64_t* remaining, uint8_t* termination,
+                       cudaStream_t s) {
+  if (count == 0) return DPA_OK;
+  if (ctx->profiling) DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->events[0], s));
+  const uint32_t* order = nullptr;
+  if (o->morton_order) {
+    const int st = build_order(ctx, field, positions, count, s, &order);
+    if (st != DPA_OK) return st;
+  }
+  if (ctx->profiling) DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->events[1], s));
+  dpa::AdvectArgs a{};
+  a.count = count;
+  a.order = order;
+  a.positions = positions;
+  a.remaining = remaining;
+  a.termination = termination;
+  a.coefficients = dpa::make_step_coefficients(o->step_size);
+  DPA_TRY_CUDA(ctx, dpa::launch_advect(field->view, a, o->integrator, false, s));
+  ctx->launches += 1;
+  if (ctx->profiling) {
+    DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->events[2], s));
+    ctx->timed_order = true;
+  }
+  return DPA_OK;
+}
+
+int exclusive_scan(dpa_context* ctx, const uint64_t* in, uint64_t* out, uint64_t count,
+                   cudaStream_t stream) {
+  size_t temp = 0;
+  DPA_TRY_CUDA(ctx, cub::DeviceScan::ExclusiveSum(nullptr, temp, in, out, int64_t(count), stream));
+  DPA_TRY_CUDA(ctx, ctx->scan_temp.reserve(temp));
+  DPA_TRY_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->scan_temp.ptr, temp, in, out,
+                                                  int64_t(count), stream));
+  return DPA_OK;
+}
+
+// Advects and emits particles [begin, end) of a recording round. The device
+// arrays ctx->positions / remaining hold the whole round.
+int record_piece(dpa_context* ctx, const dpa_field* field, const dpa_advect_options* o,
+                 const dpa::StepCoefficients& k, uint64_t begin, uint64_t end,
+                 const uint64_t* host_remaining, uint64_t* round_vertices,
+                 uint64_t* round_indices, bool final_piece, dpa_curve_sink sink, void* user) {
+  cudaStream_t s = ctx->stream;
+  const uint64_t n = end - begin;
+  // Raw (unpruned) vertex offsets: remaining + 2 slots per particle.
+  std::vector<uint64_t> offsets(n);
+  uint64_t raw_total = 0;
+  for (uint64_t i = 0; i < n; ++i) {
+    offsets[i] = raw_total;
+    raw_total += host_remaining[begin + i] + 2;
+  }
+  DPA_TRY_CUDA(ctx, ctx->raw.reserve(raw_total * 12));
+  DPA_TRY_CUDA(ctx, ctx->raw_offsets.reserve(n * 8));
+  DPA_TRY_CUDA(ctx, ctx->raw_counts.reserve(n * 8));
+  DPA_TRY_CUDA(ctx, ctx->kept_vertices.reserve(n * 4));
+  DPA_TRY_CUDA(ctx, ctx->kept_segments.reserve(n * 4));
+  DPA_TRY_CUDA(ctx, ctx->wide.reserve(n * 8));
+  DPA_TRY_CUDA(ctx, ctx->vertex_offsets.reserve(n * 8));
+  DPA_TRY_CUDA(ctx, ctx->segment_offsets.reserve(n * 8));
+  DPA_TRY_CUDA(ctx, ctx->totals.reserve(32));
+  DPA_TRY_CUDA(ctx, ctx->host_totals.reserve(32));
+  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->raw_offsets.ptr, offsets.data(), n * 8,
+                                    cudaMemcpyHostToDevice, s));
+
+  float* positions = ctx->positions.as<float>() + 3 * begin;
+  uint64_t* remaining = ctx->remaining.as<uint64_t>() + begin;
+  uint8_t* termination = ctx->termination.as<uint8_t>() + begin;
+  const uint32_t* order = nullptr;
+  if (o->morton_order) {
+    const int st = build_order(ctx, field, positions, n, s, &order);
+    if (st != DPA_OK) return st;
+  }
+  dpa::AdvectArgs a{};
+  a.count = n;
+  a.order = order;
+  a.positions = positions;
+  a.remaining = remaining;
+  a.termination = termination;
+  a.coefficients = k;
+  a.raw_vertices = ctx->raw.as<float>();
+  a.raw_offsets = ctx->raw_offsets.as<uint64_t>();
+  a.kept_vertices = ctx->kept_vertices.as<uint32_t>();
+  a.kept_segments = ctx->kept_segments.as<uint32_t>();
+  DPA_TRY_CUDA(ctx, dpa::launch_advect(field->view, a, o->integrator, true, s));
+  ctx->launches += 1;
+
+  // Per-particle raw counts, then piece-local offsets of kept vertices and
+  // kept segments.
+  DPA_TRY_CUDA(ctx, dpa::launch_raw_counts(ctx->remaining_in.as<uint64_t>() + begin, remaining, n,
+                                           ctx->raw_counts.as<uint64_t>(), s));
+  DPA_TRY_CUDA(ctx, dpa::launch_widen_u32(ctx->kept_vertices.as<uint32_t>(), n,
+                                          ctx->wide.as<uint64_t>(), s));
+  int st = exclusive_scan(ctx, ctx->wide.as<uint64_t>(), ctx->vertex_offsets.as<uint64_t>(), n, s);
+  if (st != DPA_OK) return st;
+  DPA_TRY_CUDA(ctx, dpa::launch_widen_u32(ctx->kept_segments.as<uint32_t>(), n,
+                                          ctx->wide.as<uint64_t>(), s));
+  st = exclusive_scan(ctx, ctx->wide.as<uint64_t>(), ctx->segment_offsets.as<uint64_t>(), n, s);
+  if (st != DPA_OK) return st;
+
+  uint64_t* ht = ctx->host_totals.as<uint64_t>();
+  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ht, ctx->vertex_offsets.as<uint64_t>() + (n - 1), 8,
+                                    cudaMemcpyDeviceToHost, s));
+  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ht + 1, ctx->segment_offsets.as<uint64_t>() + (n - 1), 8,
+                                    cudaMemcpyDeviceToHost, s));
+  uint32_t* last_counts = ctx->host_totals.as<uint32_t>() + 4;
+  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(&last_counts[0], ctx->kept_vertices.as<uint32_t>() + (n - 1), 4,
+                                    cudaMemcpyDeviceToHost, s));
+  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(&last_counts[1], ctx->kept_segments.as<uint32_t>() + (n - 1), 4,
+                                    cudaMemcpyDeviceToHost, s));
+  DPA_TRY_CUDA(ctx, cudaStreamSynchronize(s));
+  const uint64_t piece_vertices = ht[0] + last_counts[0];
+  const uint64_t piece_segments = ht[1] + last_counts[1];
+  const uint64_t piece_indices = 2 * piece_segments;
+  if (!o->index64 && *round_vertices + piece_vertices > 0xffffffffull)
+    return fail(ctx, DPA_ERROR_UNSUPPORTED,
+                "the round's curve has more vertices than 32-bit indices can address; "
+                "set index64");
+
+  const size_t index_bytes = o->index64 ? 8 : 4;
+  DPA_TRY_CUDA(ctx, ctx->out_vertices.reserve(piece_vertices * 12));
+  DPA_TRY_CUDA(ctx, ctx->out_colors.reserve(piece_vertices * 4));
+  DPA_TRY_CUDA(ctx, ctx->out_indices.reserve(piece_indices * index_bytes));
+  DPA_TRY_CUDA(ctx, ctx->host_vertices.reserve(piece_vertices * 12));
+  DPA_TRY_CUDA(ctx, ctx->host_colors.reserve(piece_vertices * 4));
+  DPA_TRY_CUDA(ctx, ctx->host_indices.reserve(piece_indices * index_bytes));
+
+  dpa::EmitArgs e{};
+  e.count = n;
+  e.raw_vertices = ctx->raw.as<float>();
+  e.raw_offsets = ctx->raw_offsets.as<uint64_t>();
+  e.steps_raw = ctx->raw_counts.as<uint64_t>();
+  e.vertex_offsets = ctx->vertex_offsets.as<uint64_t>();
+  e.segment_offsets = ctx->segment_offsets.as<uint64_t>();
+  e.kept_vertices = ctx->kept_vertices.as<uint32_t>();
+  e.vertex_base = *round_vertices;
+  e.vertices = ctx->out_vertices.as<float>();
+  e.colors = o->colors ? ctx->out_colors.as<float>() : nullptr;
+  e.indices = ctx->out_indices.ptr;
+  DPA_TRY_CUDA(ctx, dpa::launch_emit(e, o->index64 != 0, o->colors != 0, s));
+  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->host_vertices.ptr, ctx->out_vertices.ptr,
+                                    piece_vertices * 12, cudaMemcpyDeviceToHost, s));
+  if (o->colors)
+    DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->host_colors.ptr, ctx->out_colors.ptr,
+                                      piece_vertices * 4, cudaMemcpyDeviceToHost, s));
+  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->host_indices.ptr, ctx->out_indices.ptr,
+                                    piece_indices * index_bytes, cudaMemcpyDeviceToHost, s));
+  DPA_TRY_CUDA(ctx, cudaStreamSynchronize(s));
+
+  if (sink) {
+    dpa_curve_chunk c{};
+    c.vertex_offset = *round_vertices;
+    c.vertex_count = piece_vertices;
+    c.vertices = ctx->host_vertices.as<float>();
+    c.colors = o->colors ? ctx->host_colors.as<float>() : nullptr;
+    c.index_offset = *round_indices;
+    c.index_count = piece_indices;
+    c.indices = ctx->host_indices.ptr;
+    c.last = final_piece ? 1 : 0;
+    if (sink(user, &c) != 0) return fail(ctx, DPA_ERROR_SINK, "curve sink aborted the round");
+  }
+  *round_vertices += piece_vertices;
+  *round_indices += piece_indices;
+  return DPA_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* dpa_version(void) { return "dpa_b200 0.1.0 (sm_100a)"; }
+
+int dpa_device_count(int* count) {
+  if (!count) return DPA_ERROR_INVALID_ARGUMENT;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+    cudaGetLastError();
+    n = 0;
+  }
+  *count = n;
+  return DPA_OK;
+}
+
+int dpa_context_create(int device, dpa_context** out) {
+  if (!out) return DPA_ERROR_INVALID_ARGUMENT;
+  *out = nullptr;
+  return guarded(nullptr, [&]() -> int {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || device < 0 || device >= n) {
+      cudaGetLastError();
+      return DPA_ERROR_CUDA;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) return DPA_ERROR_CUDA;
+    dpa_context* ctx = new dpa_context();
+    ctx->device = device;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      delete ctx;
+      return DPA_ERROR_CUDA;
+    }
+    *out = ctx;
+    return DPA_OK;
+  });
+}
+
+int dpa_context_destroy(dpa_context* ctx) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  ctx->release_all();
+  for (cudaEvent_t e : ctx->events)
+    if (e) cudaEventDestroy(e);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return DPA_OK;
+}
+
+const char* dpa_last_error(const dpa_context* ctx) {
+  if (!ctx) return "no context";
+  return ctx->error.c_str();
+}
+
+void* dpa_context_stream(dpa_context* ctx) { return ctx ? static_cast<void*>(ctx->stream) : nullptr; }
+
+int dpa_context_synchronize(dpa_context* ctx) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+  DPA_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  return DPA_OK;
+}
+
+int dpa_context_set_staging_limit(dpa_context* ctx, uint64_t bytes) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  if (bytes < 4096) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "staging limit below 4 KiB");
+  ctx->staging_limit = bytes;
+  return DPA_OK;
+}
+
+int dpa_context_set_profiling(dpa_context* ctx, int32_t enabled) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+  if (enabled && !ctx->events[0])
+    for (cudaEvent_t& e : ctx->events) DPA_TRY_CUDA(ctx, cudaEventCreate(&e));
+  ctx->profiling = enabled != 0;
+  ctx->timed_order = false;
+  return DPA_OK;
+}
+
+int dpa_context_last_timing(dpa_context* ctx, float* order_ms, float* advect_ms) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  if (!ctx->profiling || !ctx->timed_order)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "no profiled advection since profiling was enabled");
+  DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+  DPA_TRY_CUDA(ctx, cudaEventSynchronize(ctx->events[2]));
+  float a = 0.0f, b = 0.0f;
+  DPA_TRY_CUDA(ctx, cudaEventElapsedTime(&a, ctx->events[0], ctx->events[1]));
+  DPA_TRY_CUDA(ctx, cudaEventElapsedTime(&b, ctx->events[1], ctx->events[2]));
+  if (order_ms) *order_ms = a;
+  if (advect_ms) *advect_ms = b;
+  return DPA_OK;
+}
+
+int dpa_context_launch_count(const dpa_context* ctx, uint64_t* launches) {
+  if (!ctx || !launches) return DPA_ERROR_INVALID_ARGUMENT;
+  *launches = ctx->launches;
+  return DPA_OK;
+}
+
+int dpa_integrator_from_name(const char* name, int32_t* integrator) {
+  if (!name || !integrator) return DPA_ERROR_INVALID_ARGUMENT;
+  static const struct {
+    const char* name;
+    int32_t code;
+  } table[] = {
+      {"euler", DPA_INTEGRATOR_EULER},
+      {"modified_midpoint", DPA_INTEGRATOR_MODIFIED_MIDPOINT},
+      {"runge_kutta_4", DPA_INTEGRATOR_RUNGE_KUTTA_4},
+      {"runge_kutta_cash_karp_54", DPA_INTEGRATOR_RUNGE_KUTTA_CASH_KARP_54},
+      {"runge_kutta_dormand_prince_5", DPA_INTEGRATOR_RUNGE_KUTTA_DORMAND_PRINCE_5},
+      {"runge_kutta_fehlberg_78", DPA_INTEGRATOR_RUNGE_KUTTA_FEHLBERG_78},
+      {"adams_bashforth_2", DPA_INTEGRATOR_ADAMS_BASHFORTH_2},
+      {"adams_bashforth_moulton_2", DPA_INTEGRATOR_ADAMS_BASHFORTH_MOULTON_2},
+      {"runge_kutta_4_true", DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE},
+  };
+  for (const auto& e : table) {
+    if (std::strcmp(e.name, name) == 0) {
+      *integrator = e.code;
+      return DPA_OK;
+    }
+  }
+  return DPA_ERROR_INVALID_ARGUMENT;
+}
+
+static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
+                        const uint64_t shape[3], const float offset[3], const float spacing[3],
+                        int32_t storage, dpa_field** out) {
+  if (!ctx || !out || !shape || !offset || !spacing)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "NULL argument");
+  *out = nullptr;
+  if (storage != DPA_STORAGE_F32 && storage != DPA_STORAGE_F16 && storage != DPA_STORAGE_BF16)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "unknown storage");
+  for (int i = 0; i < 3; ++i) {
+    if (shape[i] == 0 || shape[i] > (1u << 24))
+      return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "field shape must be in [1, 2^24] per axis");
+    if (!(spacing[i] > 0.0f) || !std::isfinite(spacing[i]) || !std::isfinite(offset[i]))
+      return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "spacing must be positive and finite");
+  }
+  const uint64_t nodes = shape[0] * shape[1] * shape[2];
+  if (nodes > (1ull << 33)) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "field too large");
+  if (nodes && !xyzv) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "field data is NULL");
+  return guarded(ctx, [&]() -> int {
+    DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    dpa_field* f = new dpa_field();
+    f->owner = ctx;
+    f->storage = storage;
+    const size_t node_bytes = storage == DPA_STORAGE_F32 ? 16 : 8;
+    cudaError_t e = f->nodes.reserve(nodes * node_bytes);
+    const float* src = xyzv;
+    DeviceBuffer staging;
+    if (e == cudaSuccess && !device_input) {
+      e = staging.reserve(nodes * 12);
+      if (e == cudaSuccess)
+        e = cudaMemcpyAsync(staging.ptr, xyzv, nodes * 12, cudaMemcpyHostToDevice, ctx->stream);
+      src = staging.as<float>();
+    }
+    if (e == cudaSuccess) e = dpa::launch_repack(src, nodes, storage, f->nodes.ptr, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    staging.release();
+    if (e != cudaSuccess) {
+      f->nodes.release();
+      delete f;
+      return fail_cuda(ctx, e, "field upload");
+    }
+    bool pow2 = true;
+    for (int i = 0; i < 3; ++i) {
+      f->shape[i] = shape[i];
+      f->offset[i] = offset[i];
+      f->spacing[i] = spacing[i];
+      pow2 = pow2 && is_power_of_two(spacing[i]);
+    }
+    dpa::FieldView& v = f->view;
+    v.nodes = f->nodes.ptr;
+    for (int i = 0; i < 3; ++i) {
+      v.n[i] = int32_t(shape[i]);
+      v.offset[i] = offset[i];
+      v.spacing[i] = spacing[i];
+      v.inv_spacing[i] = 1.0f / spacing[i];
+      v.limit[i] = float(int64_t(shape[i]) - 2);
+    }
+    v.stride0 = int64_t(shape[1]) * int64_t(shape[2]);
+    v.stride1 = int32_t(shape[2]);
+    v.storage = storage;
+    v.pow2 = pow2 ? 1 : 0;
+    *out = f;
+    return DPA_OK;
+  });
+}
+
+int dpa_field_create(dpa_context* ctx, const float* xyzv, const uint64_t shape[3],
+                     const float offset[3], const float spacing[3], int32_t storage,
+                     dpa_field** out) {
+  return create_field(ctx, xyzv, false, shape, offset, spacing, storage, out);
+}
+
+int dpa_field_create_device(dpa_context* ctx, const float* device_xyzv, const uint64_t shape[3],
+                            const float offset[3], const float spacing[3], int32_t storage,
+                            dpa_field** out) {
+  return create_field(ctx, device_xyzv, true, shape, offset, spacing, storage, out);
+}
+
+int dpa_field_destroy(dpa_context* ctx, dpa_field* field) {
+  if (!ctx || !field) return DPA_ERROR_INVALID_ARGUMENT;
+  if (field->owner != ctx) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "field belongs to another context");
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  field->nodes.release();
+  delete field;
+  return DPA_OK;
+}
+
+int dpa_field_info(const dpa_field* field, uint64_t shape[3], float offset[3], float spacing[3],
+                   int32_t* storage, uint64_t* device_bytes) {
+  if (!field) return DPA_ERROR_INVALID_ARGUMENT;
+  for (int i = 0; i < 3; ++i) {
+    if (shape) shape[i] = field->shape[i];
+    if (offset) offset[i] = field->offset[i];
+    if (spacing) spacing[i] = field->spacing[i];
+  }
+  if (storage) *storage = field->storage;
+  if (device_bytes) *device_bytes = field->nodes.bytes;
+  return DPA_OK;
+}
+
+int dpa_advect_round(dpa_context* ctx, const dpa_field* field, const dpa_advect_options* options,
+                     uint64_t count, float* positions, uint64_t* remaining,
+                     uint8_t* termination, dpa_curve_sink sink, void* sink_user) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  int st = check_options(ctx, options);
+  if (st != DPA_OK) return st;
+  if (!field || field->owner != ctx) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "bad field");
+  if (count && (!positions || !remaining))
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "positions or remaining is NULL");
+  if (count > 0xffffffffull)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "at most 2^32-1 particles per round");
+  return guarded(ctx, [&]() -> int {
+    DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    const dpa::StepCoefficients k = dpa::make_step_coefficients(options->step_size);
+    if (options->record) {
+      for (uint64_t i = 0; i < count; ++i)
+        if (remaining[i] > 0xfffffff0ull)
+          return fail(ctx, DPA_ERROR_INVALID_ARGUMENT,
+                      "recording supports at most 2^32-16 iterations per particle");
+    }
+    if (count == 0) {
+      if (options->record && sink) {
+        dpa_curve_chunk c{};
+        c.last = 1;
+        if (sink(sink_user, &c) != 0) return fail(ctx, DPA_ERROR_SINK, "curve sink aborted the round");
+      }
+      return DPA_OK;
+    }
+    DPA_TRY_CUDA(ctx, ctx->positions.reserve(count * 12));
+    DPA_TRY_CUDA(ctx, ctx->remaining.reserve(count * 8));
+    DPA_TRY_CUDA(ctx, ctx->termination.reserve(count));
+    DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->positions.ptr, positions, count * 12,
+                                      cudaMemcpyHostToDevice, s));
+    DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->remaining.ptr, remaining, count * 8,
+                                      cudaMemcpyHostToDevice, s));
+    if (!options->record) {
+      st = advect_device_impl(ctx, field, options, count, ctx->positions.as<float>(),
+                              ctx->remaining.as<uint64_t>(), ctx->termination.as<uint8_t>(), s);
+      if (st != DPA_OK) return st;
+    } else {
+      DPA_TRY_CUDA(ctx, ctx->remaining_in.reserve(count * 8));
+      DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->remaining_in.ptr, ctx->remaining.ptr, count * 8,
+                                        cudaMemcpyDeviceToDevice, s));
+      // Pieces of the round whose unpruned curves fit the staging limit.
+      const uint64_t limit_vertices = std::max<uint64_t>(ctx->staging_limit / 12, 1);
+      uint64_t round_vertices = 0, round_indices = 0;
+      uint64_t begin = 0;
+      while (begin < count) {
+        uint64_t end = begin, raw = 0;
+        while (end < count && (end == begin || raw + remaining[end] + 2 <= limit_vertices)) {
+          raw += remaining[end] + 2;
+          ++end;
+        }
+        st = record_piece(ctx, field, options, k, begin, end, remaining, &round_vertices,
+                          &round_indices, end == count, sink, sink_user);
+        if (st != DPA_OK) return st;
+        begin = end;
+      }
+    }
+    DPA_TRY_CUDA(ctx, cudaMemcpyAsync(positions, ctx->positions.ptr, count * 12,
+                                      cudaMemcpyDeviceToHost, s));
+    DPA_TRY_CUDA(ctx, cudaMemcpyAsync(remaining, ctx->remaining.ptr, count * 8,
+                                      cudaMemcpyDeviceToHost, s));
+    if (termination)
+      DPA_TRY_CUDA(ctx, cudaMemcpyAsync(termination, ctx->termination.ptr, count,
+                                        cudaMemcpyDeviceToHost, s));
+    DPA_TRY_CUDA(ctx, cudaStreamSynchronize(s));
+    return DPA_OK;
+  });
+}
+
+int dpa_advect_device(dpa_context* ctx, const dpa_field* field, const dpa_advect_options* options,
+                      uint64_t count, float* device_positions, uint64_t* device_remaining,
+                      uint8_t* device_termination, void* stream) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  int st = check_options(ctx, options);
+  if (st != DPA_OK) return st;
+  if (options->record)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT,
+                "dpa_advect_device does not record; use dpa_advect_round");
+  if (!field || field->owner != ctx) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "bad field");
+  if (count && (!device_positions || !device_remaining))
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "positions or remaining is NULL");
+  if (count > 0xffffffffull)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "at most 2^32-1 particles per call");
+  return guarded(ctx, [&]() -> int {
+    DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    return advect_device_impl(ctx, field, options, count, device_positions, device_remaining,
+                              device_termination, pick_stream(ctx, stream));
+  });
+}
+
+int dpa_seed_lattice_device(dpa_context* ctx, const float offset_in[3], const float size_in[3],
+                            const float stride[3], const float* aabb, uint64_t* count,
+                            uint64_t shape_out[3], float* device_positions, void* stream) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  if (!offset_in || !size_in || !stride || !count)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "NULL argument");
+  float offset[3] = {offset_in[0], offset_in[1], offset_in[2]};
+  float size[3] = {size_in[0], size_in[1], size_in[2]};
+  uint64_t shape[3] = {0, 0, 0};
+  bool empty = false;
+  if (aabb) {
+    // Eigen AlignedBox intersection and isEmpty (uniform_seed_generator.cpp:18-27).
+    float lo[3], hi[3];
+    for (int i = 0; i < 3; ++i) {
+      lo[i] = std::max(aabb[i], offset[i]);
+      hi[i] = std::min(aabb[3 + i], offset[i] + size[i]);
+      if (lo[i] > hi[i]) empty = true;
+    }
+    if (!empty)
+      for (int i = 0; i < 3; ++i) {
+        offset[i] = lo[i];
+        size[i] = hi[i] - lo[i];
+      }
+  }
+  if (!empty)
+    for (int i = 0; i < 3; ++i) {
+      if (!(stride[i] > 0.0f)) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "stride must be positive");
+      const float q = size[i] / stride[i];
+      shape[i] = q > 0.0f ? uint64_t(q) : 0;
+    }
+  *count = shape[0] * shape[1] * shape[2];
+  if (shape_out)
+    for (int i = 0; i < 3; ++i) shape_out[i] = shape[i];
+  if (!device_positions || *count == 0) return DPA_OK;
+  return guarded(ctx, [&]() -> int {
+    DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    DPA_TRY_CUDA(ctx, dpa::launch_lattice_seeds(offset, stride, shape, device_positions,
+                                                pick_stream(ctx, stream)));
+    return DPA_OK;
+  });
+}
+
+static int ftle_common(dpa_context* ctx, const dpa_field* field, const float seed_stride[3],
+                       uint64_t iterations, float step_size, uint64_t count,
+                       const float* original, const float* final_positions, int32_t mapping,
+                       float* ftle, uint64_t shape_out[3], cudaStream_t s, dpa::FtleArgs* a,
+                       uint64_t* cells) {
+  if (!field || field->owner != ctx) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "bad field");
+  if (!seed_stride) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "seed_stride is NULL");
+  if (mapping != DPA_FTLE_MAPPING_REFERENCE && mapping != DPA_FTLE_MAPPING_LATTICE)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "unknown FTLE mapping");
+  (void)s;
+  for (int i = 0; i < 3; ++i) {
+    if (!(seed_stride[i] > 0.0f)) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "stride must be positive");
+    // size(scalar(shape) / stride) (ftle_estimator.cpp:16-22).
+    const float q = float(field->shape[i]) / seed_stride[i];
+    a->shape[i] = q > 0.0f ? uint64_t(q) : 0;
+    a->offset[i] = field->offset[i];
+    a->spacing[i] = field->spacing[i] * seed_stride[i];
+    a->two_spacing[i] = 2.0f * a->spacing[i];
+  }
+  if (shape_out)
+    for (int i = 0; i < 3; ++i) shape_out[i] = a->shape[i];
+  *cells = a->shape[0] * a->shape[1] * a->shape[2];
+  if (mapping == DPA_FTLE_MAPPING_LATTICE && count != *cells)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "lattice mapping needs one particle per cell");
+  if (count && (!original || !final_positions))
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "positions are NULL");
+  (void)ftle;
+  const float horizon = std::fabs(step_size * float(iterations));
+  a->count = count;
+  a->mapping = mapping;
+  a->horizon = double(horizon);
+  return DPA_OK;
+}
+
+int dpa_ftle_estimate(dpa_context* ctx, const dpa_field* field, const float seed_stride[3],
+                      uint64_t iterations, float step_size, uint64_t count,
+                      const float* original_positions, const float* final_positions,
+                      int32_t mapping, float* ftle, uint64_t shape_out[3]) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  return guarded(ctx, [&]() -> int {
+    dpa::FtleArgs a{};
+    uint64_t cells = 0;
+    int st = ftle_common(ctx, field, seed_stride, iterations, step_size, count, original_positions,
+                         final_positions, mapping, ftle, shape_out, ctx->stream, &a, &cells);
+    if (st != DPA_OK || !ftle || cells == 0) return st;
+    DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    DPA_TRY_CUDA(ctx, ctx->ftle_original.reserve(count * 12));
+    DPA_TRY_CUDA(ctx, ctx->ftle_final.reserve(count * 12));
+    DPA_TRY_CUDA(ctx, ctx->ftle_winners.reserve(cells * 8));
+    DPA_TRY_CUDA(ctx, ctx->ftle_flow.reserve(cells * 12));
+    DPA_TRY_CUDA(ctx, ctx->ftle_out.reserve(cells * 4));
+    if (count) {
+      DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->ftle_original.ptr, original_positions, count * 12,
+                                        cudaMemcpyHostToDevice, s));
+      DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->ftle_final.ptr, final_positions, count * 12,
+                                        cudaMemcpyHostToDevice, s));
+    }
+    a.original_positions = ctx->ftle_original.as<float>();
+    a.final_positions = ctx->ftle_final.as<float>();
+    a.winners = ctx->ftle_winners.as<unsigned long long>();
+    a.flow = ctx->ftle_flow.as<float>();
+    a.ftle = ctx->ftle_out.as<float>();
+    DPA_TRY_CUDA(ctx, dpa::launch_ftle(a, s));
+    DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ftle, ctx->ftle_out.ptr, cells * 4, cudaMemcpyDeviceToHost, s));
+    DPA_TRY_CUDA(ctx, cudaStreamSynchronize(s));
+    return DPA_OK;
+  });
+}
+
+int dpa_ftle_estimate_device(dpa_context* ctx, const dpa_field* field, const float seed_stride[3],
+                             uint64_t iterations, float step_size, uint64_t count,
+                             const float* device_original_positions,
+                             const float* device_final_positions, int32_t mapping,
+                             float* device_ftle, uint64_t shape_out[3], void* stream) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  return guarded(ctx, [&]() -> int {
+    cudaStream_t s = pick_stream(ctx, stream);
+    dpa::FtleArgs a{};
+    uint64_t cells = 0;
+    int st = ftle_common(ctx, field, seed_stride, iterations, step_size, count,
+                         device_original_positions, device_final_positions, mapping, device_ftle,
+                         shape_out, s, &a, &cells);
+    if (st != DPA_OK || !device_ftle || cells == 0) return st;
+    DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    DPA_TRY_CUDA(ctx, ctx->ftle_winners.reserve(cells * 8));
+    DPA_TRY_CUDA(ctx, ctx->ftle_flow.reserve(cells * 12));
+    a.original_positions = device_original_positions;
+    a.final_positions = device_final_positions;
+    a.winners = ctx->ftle_winners.as<unsigned long long>();
+    a.flow = ctx->ftle_flow.as<float>();
+    a.ftle = device_ftle;
+    DPA_TRY_CUDA(ctx, dpa::launch_ftle(a, s));
+    return DPA_OK;
+  });
+}
+
+}  // extern "C"

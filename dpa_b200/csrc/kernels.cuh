@@ -1,0 +1,83 @@
+// kernels.cuh -- kernel argument blocks and launchers shared by the .cu files.
+#pragma once
+
+#include "common.cuh"
+
+namespace dpa {
+
+constexpr int kAdvectBlock = 256;
+
+struct AdvectArgs {
+  uint64_t count;
+  const uint32_t* order;  // processing order (Morton); null = identity
+  float* positions;       // [count][3], updated in place
+  uint64_t* remaining;    // [count], updated in place
+  uint8_t* termination;   // [count] or null
+  StepCoefficients coefficients;
+  // Recording only.
+  float* raw_vertices;          // unpruned curve of particle k at raw_offsets[k]
+  const uint64_t* raw_offsets;  // exclusive scan of remaining + 2
+  uint32_t* kept_vertices;      // per particle: vertices surviving the prune
+  uint32_t* kept_segments;      // per particle: index pairs it contributes
+};
+
+cudaError_t launch_advect(const FieldView& f, const AdvectArgs& a, int integrator, bool record,
+                          cudaStream_t stream);
+
+// Processing order: a counting sort of the particles by the Morton code of
+// their start cell on a 16^3 coarsening of the grid (four kernels). Within a
+// bucket the order is arbitrary; results never depend on processing order.
+constexpr int kOrderBuckets = 4096;
+constexpr int kOrderLaunches = 4;
+
+cudaError_t launch_order(const FieldView& f, const float* positions, uint64_t count,
+                         uint16_t* buckets, uint32_t* counts, uint32_t* order, cudaStream_t stream);
+
+struct EmitArgs {
+  uint64_t count;                 // particles in this piece, in round order
+  const float* raw_vertices;
+  const uint64_t* raw_offsets;    // per particle
+  const uint64_t* steps_raw;      // per particle: raw vertex count (steps + 2)
+  const uint64_t* vertex_offsets; // exclusive scan of kept vertices (piece-local)
+  const uint64_t* segment_offsets;// exclusive scan of kept segments (piece-local)
+  const uint32_t* kept_vertices;
+  uint64_t vertex_base;           // round-level index of the piece's first vertex
+  float* vertices;                // piece output
+  float* colors;                  // piece output or null
+  void* indices;                  // piece output (uint32 or uint64)
+};
+
+cudaError_t launch_emit(const EmitArgs& e, bool index64, bool colors, cudaStream_t stream);
+
+// Raw vertex count per particle: remaining_in - remaining_out + 2.
+cudaError_t launch_raw_counts(const uint64_t* remaining_in, const uint64_t* remaining_out,
+                              uint64_t count, uint64_t* raw_counts, cudaStream_t stream);
+
+cudaError_t launch_widen_u32(const uint32_t* in, uint64_t count, uint64_t* out,
+                             cudaStream_t stream);
+
+// Field repack: XYZV float [n][3] -> 4-wide nodes in the given storage.
+cudaError_t launch_repack(const float* xyzv, uint64_t nodes, int storage, void* out,
+                          cudaStream_t stream);
+
+struct FtleArgs {
+  uint64_t count;
+  const float* original_positions;
+  const float* final_positions;
+  int mapping;
+  uint64_t shape[3];       // flow-map lattice
+  float offset[3];
+  float spacing[3];        // field spacing * stride
+  float two_spacing[3];
+  double horizon;          // |step_size * iterations| as the reference rounds it
+  unsigned long long* winners;  // [cells], scratch
+  float* flow;             // [cells][3], scratch
+  float* ftle;             // [cells]
+};
+
+cudaError_t launch_ftle(const FtleArgs& a, cudaStream_t stream);
+
+cudaError_t launch_lattice_seeds(const float offset[3], const float stride[3],
+                                 const uint64_t shape[3], float* out, cudaStream_t stream);
+
+}  // namespace dpa

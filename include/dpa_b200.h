@@ -1,0 +1,229 @@
+/*
+ * dpa_b200.h -- C ABI of the B200 (sm_100a) advection library.
+ *
+ * This library replaces the advection stage of VRGroupRWTH/dpa: the per-round
+ * particle integration of particle_advector (source/stages/particle_advector.cpp),
+ * its curve pruning, the index and color post-passes and the FTLE estimator.
+ * Plain pointers and sizes only; every entry point returns a dpa_status and
+ * nothing throws across this boundary. A context is bound to one device and is
+ * not re-entrant: use one context per host thread.
+ *
+ * Array conventions (C-order, little endian):
+ *   field       float [n0][n1][n2][3]   the reference's XYZV dataset
+ *               (regular_grid_loader.cpp:65-88 reads it into boost::multi_array)
+ *   positions   float [count][3]        particle_3d::position (particle.hpp:70)
+ *   remaining   uint64 [count]          particle_3d::remaining_iterations
+ *   termination uint8 [count]           dpa_termination per particle
+ */
+#ifndef DPA_B200_H
+#define DPA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct dpa_context dpa_context;
+typedef struct dpa_field dpa_field;
+
+typedef enum dpa_status {
+  DPA_OK = 0,
+  DPA_ERROR_INVALID_ARGUMENT = 1,
+  DPA_ERROR_UNSUPPORTED = 2,
+  DPA_ERROR_OUT_OF_MEMORY = 3,
+  DPA_ERROR_CUDA = 4,
+  DPA_ERROR_SINK = 5,
+  DPA_ERROR_INTERNAL = 6
+} dpa_status;
+
+/* Device storage of a field. F32 keeps the reference's values exactly; F16 and
+ * BF16 halve the gather bytes and interpolate in FP32. */
+typedef enum dpa_storage {
+  DPA_STORAGE_F32 = 0,
+  DPA_STORAGE_F16 = 1,
+  DPA_STORAGE_BF16 = 2
+} dpa_storage;
+
+/* Integrators. Codes 0-7 follow the alternatives of the reference's
+ * variant_integrator (include/dpa/types/integrators.hpp:31-39) and the names
+ * of particle_advector.cpp:29-36. The GPU implements euler and
+ * runge_kutta_4; the others return DPA_ERROR_UNSUPPORTED.
+ * DPA_INTEGRATOR_RUNGE_KUTTA_4 has the reference's semantics: its system
+ * functor (particle_advector.cpp:369) samples the field once per step, so all
+ * four stages see the same derivative. DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE
+ * samples at all four stages (no counterpart in the reference). */
+typedef enum dpa_integrator {
+  DPA_INTEGRATOR_EULER = 0,
+  DPA_INTEGRATOR_MODIFIED_MIDPOINT = 1,
+  DPA_INTEGRATOR_RUNGE_KUTTA_4 = 2,
+  DPA_INTEGRATOR_RUNGE_KUTTA_CASH_KARP_54 = 3,
+  DPA_INTEGRATOR_RUNGE_KUTTA_DORMAND_PRINCE_5 = 4,
+  DPA_INTEGRATOR_RUNGE_KUTTA_FEHLBERG_78 = 5,
+  DPA_INTEGRATOR_ADAMS_BASHFORTH_2 = 6,
+  DPA_INTEGRATOR_ADAMS_BASHFORTH_MOULTON_2 = 7,
+  DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE = 100
+} dpa_integrator;
+
+/* Why a particle stopped (particle_advector.cpp:336-395). */
+typedef enum dpa_termination {
+  DPA_TERMINATION_COMPLETE = 0,      /* remaining_iterations reached 0 */
+  DPA_TERMINATION_OUT_OF_BOUNDS = 1, /* regular_grid::contains failed */
+  DPA_TERMINATION_ZERO_VELOCITY = 2  /* interpolated vector isZero() */
+} dpa_termination;
+
+/* FTLE scatter rule. REFERENCE puts each final position into the flow-map
+ * cell of floor((original_position - offset) / (spacing * stride)) exactly as
+ * ftle_estimator.cpp:39-43 does (rounding can map two seeds to one cell; the
+ * larger particle index then wins, and unmapped cells stay zero). LATTICE puts
+ * particle i into flat cell i (count must equal the lattice size). */
+typedef enum dpa_ftle_mapping {
+  DPA_FTLE_MAPPING_REFERENCE = 0,
+  DPA_FTLE_MAPPING_LATTICE = 1
+} dpa_ftle_mapping;
+
+typedef struct dpa_advect_options {
+  int32_t integrator;   /* dpa_integrator */
+  float   step_size;    /* particle_advector_step_size */
+  int32_t record;       /* particle_advector_record: emit the round's curve */
+  int32_t index64;      /* 64-bit indices (pipeline.cpp:155 decides) */
+  int32_t colors;       /* emit angular-velocity colors with the curve */
+  int32_t morton_order; /* process particles in Morton order of their start cell */
+} dpa_advect_options;
+
+/* One piece of a round's curve, delivered in order. The round's curve is the
+ * reference's integral_curve after advect, prune_integral_curves,
+ * index_generator::generate and color_generator::generate_from_angular_velocities
+ * (particle_advector.cpp:402-408, index_generator.cpp:10-39,
+ * color_generator.cpp:37-58). Index values are positions in the round's whole
+ * vertex array. Pointers are host memory owned by the library and valid only
+ * during the callback. */
+typedef struct dpa_curve_chunk {
+  uint64_t     vertex_offset; /* first vertex of this chunk within the round */
+  uint64_t     vertex_count;
+  const float* vertices;      /* vertex_count * 3 */
+  const float* colors;        /* vertex_count, or NULL when colors are off */
+  uint64_t     index_offset;  /* first index of this chunk within the round */
+  uint64_t     index_count;
+  const void*  indices;       /* uint32 or uint64 per dpa_advect_options.index64 */
+  int32_t      last;          /* non-zero on the round's final chunk */
+} dpa_curve_chunk;
+
+/* Returns 0 to continue; any other value aborts the round with DPA_ERROR_SINK. */
+typedef int (*dpa_curve_sink)(void* user, const dpa_curve_chunk* chunk);
+
+/* ---- library and context ------------------------------------------------ */
+
+const char* dpa_version(void);
+
+/* Number of visible CUDA devices (0 when none or when the driver is absent). */
+int dpa_device_count(int* count);
+
+int dpa_context_create(int device, dpa_context** out);
+int dpa_context_destroy(dpa_context* ctx);
+
+/* Message of the last failed call on this context (never NULL). */
+const char* dpa_last_error(const dpa_context* ctx);
+
+/* The context's CUDA stream (a cudaStream_t) for callers that order their own
+ * work against the library's. */
+void* dpa_context_stream(dpa_context* ctx);
+
+int dpa_context_synchronize(dpa_context* ctx);
+
+/* Upper bound on the device bytes a recording round may stage at once; larger
+ * rounds are processed in pieces (default 1 GiB). */
+int dpa_context_set_staging_limit(dpa_context* ctx, uint64_t bytes);
+
+/* Instrumentation, the counterpart of the reference's per-round timers
+ * (pipeline.cpp:98-145, benchmark.hpp:152-158). With profiling on, every
+ * non-recording advection records CUDA events on its stream around the
+ * ordering kernels and the advection kernel; dpa_context_last_timing waits
+ * for the last call's events and returns both durations in milliseconds. */
+int dpa_context_set_profiling(dpa_context* ctx, int32_t enabled);
+int dpa_context_last_timing(dpa_context* ctx, float* order_ms, float* advect_ms);
+
+/* Number of kernels this context has launched on the advection path. */
+int dpa_context_launch_count(const dpa_context* ctx, uint64_t* launches);
+
+/* ---- integrator names ----------------------------------------------------- */
+
+/* Maps the reference's config strings (particle_advector.cpp:29-36) and
+ * "runge_kutta_4_true" to a dpa_integrator. Unknown names are an error (the
+ * reference silently keeps euler). */
+int dpa_integrator_from_name(const char* name, int32_t* integrator);
+
+/* ---- fields ---------------------------------------------------------------- */
+
+/* Replaces regular_grid_loader::load_vector_field (regular_grid_loader.cpp:65-88):
+ * uploads a host XYZV field and repacks it for the device in the given storage.
+ * offset/spacing are the grid's world offset and cell spacing. */
+int dpa_field_create(dpa_context* ctx, const float* xyzv, const uint64_t shape[3],
+                     const float offset[3], const float spacing[3], int32_t storage,
+                     dpa_field** out);
+
+/* Same, from a device pointer already in this context's device memory. */
+int dpa_field_create_device(dpa_context* ctx, const float* device_xyzv, const uint64_t shape[3],
+                            const float offset[3], const float spacing[3], int32_t storage,
+                            dpa_field** out);
+
+int dpa_field_destroy(dpa_context* ctx, dpa_field* field);
+
+int dpa_field_info(const dpa_field* field, uint64_t shape[3], float offset[3], float spacing[3],
+                   int32_t* storage, uint64_t* device_bytes);
+
+/* ---- advection --------------------------------------------------------------- */
+
+/* One advection round over host arrays: replaces particle_advector::
+ * allocate_integral_curves + advect + prune_integral_curves
+ * (particle_advector.cpp:311-408, called from pipeline.cpp:115-127) and, when
+ * recording, the index and color post-passes for that round. positions and
+ * remaining are updated in place; termination (may be NULL) receives the exit
+ * reason. With options->record, the round's curve goes to sink in order. */
+int dpa_advect_round(dpa_context* ctx, const dpa_field* field, const dpa_advect_options* options,
+                     uint64_t count, float* positions, uint64_t* remaining,
+                     uint8_t* termination, dpa_curve_sink sink, void* sink_user);
+
+/* The same round over device arrays on the given stream (NULL: the context's
+ * stream), without recording. Asynchronous: returns after enqueueing. */
+int dpa_advect_device(dpa_context* ctx, const dpa_field* field, const dpa_advect_options* options,
+                      uint64_t count, float* device_positions, uint64_t* device_remaining,
+                      uint8_t* device_termination, void* stream);
+
+/* ---- seeds ------------------------------------------------------------------- */
+
+/* Lattice seeds on the device: uniform_seed_generator::generate
+ * (uniform_seed_generator.cpp:16-45, unravel order of indexing.hpp:11-20).
+ * aabb is NULL or {min0,min1,min2,max0,max1,max2}. Writes count*3 floats to
+ * device_positions when it is not NULL; *count and shape_out receive the
+ * lattice size either way. */
+int dpa_seed_lattice_device(dpa_context* ctx, const float offset[3], const float size[3],
+                            const float stride[3], const float* aabb, uint64_t* count,
+                            uint64_t shape_out[3], float* device_positions, void* stream);
+
+/* ---- FTLE --------------------------------------------------------------------- */
+
+/* Replaces ftle_estimator::estimate (ftle_estimator.cpp:7-65): flow map of
+ * shape floor(field shape / seed_stride) with spacing field spacing *
+ * seed_stride, central-difference Jacobian with the clamped border rule of
+ * regular_grid::gradient (regular_grid.hpp:87-108), C = J^T J, FP64 largest
+ * eigenvalue and ln(sqrt(lambda)) / |step_size * iterations|. Host arrays;
+ * ftle receives product(shape_out) floats (pass NULL to query shape_out). */
+int dpa_ftle_estimate(dpa_context* ctx, const dpa_field* field, const float seed_stride[3],
+                      uint64_t iterations, float step_size, uint64_t count,
+                      const float* original_positions, const float* final_positions,
+                      int32_t mapping, float* ftle, uint64_t shape_out[3]);
+
+/* Device-array variant on the given stream (NULL: the context's stream). */
+int dpa_ftle_estimate_device(dpa_context* ctx, const dpa_field* field, const float seed_stride[3],
+                             uint64_t iterations, float step_size, uint64_t count,
+                             const float* device_original_positions,
+                             const float* device_final_positions, int32_t mapping,
+                             float* device_ftle, uint64_t shape_out[3], void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,200 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle.
+
+Bar: final positions, termination reasons and steps, pruned curve vertices
+and index buffers are bit-exact; colors agree within 2e-6 rad (atan2f of
+CUDA and of the host libm may differ in the last bits; the exact special
+cases, 0 and pi, must match exactly)."""
+import math
+
+import numpy as np
+import pytest
+
+import dpa_b200
+from dpa_b200 import ParticleAdvector, Particles, fields, seeds
+
+pytestmark = pytest.mark.gpu
+
+COLOR_ATOL = 2e-6
+
+
+def _seeds_in_box(grid, count, seed, box=None):
+    offset, size = seeds.seed_box(grid)
+    return seeds.generate_random(offset, size, count, 0, aabb=box, seed=seed).position
+
+
+def compare(ctx, oracle, grid, positions, iterations, integrator, step, ppr, record,
+            storage="f32", index64=False, morton=True, staging=None):
+    """Runs the GPU rounds and the oracle rounds on the same input."""
+    oracle_data = grid.data
+    if storage == "f16":
+        oracle_data = grid.data.astype(np.float16).astype(np.float32)
+    elif storage == "bf16":
+        import torch
+        oracle_data = torch.from_numpy(grid.data).to(torch.bfloat16).float().numpy()
+    og = oracle.OracleGrid(oracle_data, grid.spacing, grid.offset)
+    rem = np.broadcast_to(np.asarray(iterations, np.uint64), (positions.shape[0],)).copy()
+    want, want_rounds = oracle.advect_rounds(og, integrator, step, positions, rem, ppr, record,
+                                             index64)
+    if staging:
+        ctx.set_staging_limit(staging)
+    field = ctx.field(grid, storage)
+    adv = ParticleAdvector(ctx, ppr, "none", integrator, step, False, record,
+                           use_64_bit_indices=index64, morton_order=morton)
+    got = adv.advect(field, Particles.create(positions, rem))
+    if staging:
+        ctx.set_staging_limit(1 << 30)
+    np.testing.assert_array_equal(got.inactive_particles.termination, want.termination)
+    np.testing.assert_array_equal(got.inactive_particles.remaining_iterations, want.remaining)
+    np.testing.assert_array_equal(got.inactive_particles.position, want.positions)
+    if record:
+        assert len(got.integral_curves) == len(want_rounds)
+        for c, r in zip(got.integral_curves, want_rounds):
+            np.testing.assert_array_equal(c.vertices, r.vertices)
+            assert c.indices.dtype == r.indices.dtype
+            np.testing.assert_array_equal(c.indices, r.indices)
+            np.testing.assert_allclose(c.colors, r.colors, rtol=0, atol=COLOR_ATOL)
+            special = (r.colors == 0) | (r.colors == np.float32(math.pi))
+            np.testing.assert_array_equal(c.colors[special], r.colors[special])
+    return got, want
+
+
+@pytest.mark.parametrize("integrator", ["runge_kutta_4", "euler", "runge_kutta_4_true"])
+def test_abc_recording_matches_oracle(ctx, oracle, integrator):
+    grid = fields.abc(64)
+    box = ([0, 0, 0], [2 * math.pi] * 3)
+    pos = _seeds_in_box(grid, 512, 0, box)
+    compare(ctx, oracle, grid, pos, 300, integrator, 0.01, 512, True)
+
+
+def test_abc_default_seed_box_has_out_of_bounds_starts(ctx, oracle):
+    # The default seed box reaches one cell past the valid domain, so some
+    # particles leave at step 0 with a two-vertex curve.
+    grid = fields.abc(32)
+    pos = _seeds_in_box(grid, 2048, 3)
+    got, want = compare(ctx, oracle, grid, pos, 50, "runge_kutta_4", 0.05, 2048, True)
+    assert np.sum((want.termination == 1) & (want.steps == 0)) > 0
+
+
+def test_multiple_rounds_take_the_tail(ctx, oracle):
+    grid = fields.abc(32)
+    pos = _seeds_in_box(grid, 1000, 4, ([0, 0, 0], [2 * math.pi] * 3))
+    got, _ = compare(ctx, oracle, grid, pos, 80, "runge_kutta_4", 0.02, 300, True)
+    assert got.rounds == 4
+    assert [c.vertices.shape[0] > 0 for c in got.integral_curves] == [True] * 4
+
+
+def test_u64_indices_and_small_staging_pieces(ctx, oracle):
+    grid = fields.abc(32)
+    pos = _seeds_in_box(grid, 777, 5, ([0, 0, 0], [2 * math.pi] * 3))
+    compare(ctx, oracle, grid, pos, 120, "runge_kutta_4", 0.02, 777, True, index64=True,
+            staging=12 * 122 * 50)
+    compare(ctx, oracle, grid, pos, 120, "runge_kutta_4", 0.02, 777, True, index64=False,
+            staging=12 * 122 * 7)
+
+
+def test_curl_noise_power_of_two_spacing_end_positions(ctx, oracle):
+    grid = fields.curl_noise(64, 4.0, 1)
+    pos = _seeds_in_box(grid, 4096, 1)
+    got, want = compare(ctx, oracle, grid, pos, 400, "runge_kutta_4", 0.25, 4096, False)
+    assert np.sum(want.termination == 0) > 1000
+
+
+def test_non_power_of_two_unit_like_spacing(ctx, oracle):
+    grid = fields.curl_noise(48, 3.0, 9, spacing=0.7)
+    pos = _seeds_in_box(grid, 2048, 2)
+    compare(ctx, oracle, grid, pos, 200, "runge_kutta_4", 0.2, 2048, False)
+
+
+@pytest.mark.parametrize("storage", ["f16", "bf16"])
+def test_half_storage_is_exact_on_the_rounded_field(ctx, oracle, storage):
+    # The device widens 16-bit nodes to FP32 exactly and then runs the same
+    # arithmetic, so it matches the oracle on the rounded field bit for bit.
+    grid = fields.curl_noise(64, 4.0, 11)
+    pos = _seeds_in_box(grid, 2048, 6)
+    compare(ctx, oracle, grid, pos, 300, "runge_kutta_4", 0.25, 2048, False, storage=storage)
+
+
+def test_morton_order_does_not_change_results(ctx, oracle):
+    grid = fields.curl_noise(32, 3.0, 2)
+    pos = _seeds_in_box(grid, 1500, 8)
+    a, _ = compare(ctx, oracle, grid, pos, 100, "euler", 0.3, 1500, True, morton=True)
+    b, _ = compare(ctx, oracle, grid, pos, 100, "euler", 0.3, 1500, True, morton=False)
+    np.testing.assert_array_equal(a.inactive_particles.position, b.inactive_particles.position)
+
+
+def test_edge_cases(ctx, oracle):
+    grid = fields.abc(16)
+    field = ctx.field(grid)
+    # empty round
+    adv = ParticleAdvector(ctx, 10, "none", "runge_kutta_4", 0.01, False, True)
+    out = adv.advect(field, Particles.create(np.zeros((0, 3), np.float32), 10))
+    assert out.rounds == 0 and len(out.inactive_particles) == 0
+    # zero remaining, outside, NaN, exactly on the upper boundary
+    top = np.float32(grid.spacing[0] * np.float32(14))
+    pos = np.array([[1, 1, 1], [50, 1, 1], [np.nan, 1, 1], [top, 1, 1], [1, 1, 1]], np.float32)
+    rem = np.array([0, 5, 5, 5, 5], np.uint64)
+    og = oracle.OracleGrid.of(grid)
+    want = oracle.advect_round(og, "runge_kutta_4", 0.01, pos, rem, record=True)
+    got = adv.advect(field, Particles(pos.copy(), rem.copy(), pos.copy()))
+    np.testing.assert_array_equal(got.inactive_particles.termination, want.termination)
+    np.testing.assert_array_equal(got.inactive_particles.remaining_iterations, want.remaining)
+    c = got.integral_curves[0]
+    np.testing.assert_array_equal(c.vertices, want.vertices)
+    np.testing.assert_array_equal(c.indices, want.indices)
+    # zero field: zero-velocity termination at step 0
+    zero = dpa_b200.RegularGrid.from_data(np.zeros((8, 8, 8, 3), np.float32), (1, 1, 1))
+    zf = ctx.field(zero)
+    out = ParticleAdvector(ctx, 4, "none", "euler", 0.1, False, False).advect(
+        zf, Particles.create(np.full((3, 3), 2.0, np.float32), 9))
+    assert list(out.inactive_particles.termination) == [2, 2, 2]
+    assert list(out.inactive_particles.remaining_iterations) == [9, 9, 9]
+
+
+def test_unsupported_integrators_report_an_error(ctx):
+    grid = fields.abc(8)
+    field = ctx.field(grid)
+    adv = ParticleAdvector(ctx, 4, "none", "runge_kutta_dormand_prince_5", 0.1, False, False)
+    with pytest.raises(dpa_b200.DpaError) as e:
+        adv.advect(field, Particles.create(np.ones((2, 3), np.float32), 3))
+    assert e.value.status == 2
+
+
+def test_device_api_matches_host_api(ctx, oracle):
+    import ctypes as C
+    import torch
+    from dpa_b200 import _native as N
+    grid = fields.curl_noise(64, 4.0, 3)
+    pos = _seeds_in_box(grid, 3000, 9)
+    field = ctx.field(grid)
+    adv = ParticleAdvector(ctx, 3000, "none", "runge_kutta_4", 0.25, False, False)
+    host = adv.advect(field, Particles.create(pos, 200))
+    dp = torch.from_numpy(pos.copy()).cuda()
+    dr = torch.full((3000,), 200, dtype=torch.int64, device="cuda")
+    dt = torch.zeros(3000, dtype=torch.uint8, device="cuda")
+    opts = adv.options(False)
+    ctx.check(ctx._lib.dpa_advect_device(ctx.handle, field.handle, C.byref(opts), 3000,
+                                         C.c_void_p(dp.data_ptr()), C.c_void_p(dr.data_ptr()),
+                                         C.c_void_p(dt.data_ptr()), None))
+    ctx.synchronize()
+    np.testing.assert_array_equal(dp.cpu().numpy(), host.inactive_particles.position)
+    np.testing.assert_array_equal(dr.cpu().numpy().astype(np.uint64),
+                                  host.inactive_particles.remaining_iterations)
+    np.testing.assert_array_equal(dt.cpu().numpy(), host.inactive_particles.termination)
+
+
+@pytest.mark.parametrize("mapping", ["reference", "lattice"])
+def test_ftle_matches_oracle(ctx, oracle, mapping):
+    grid = fields.abc_perturbed(64, seed=2)
+    field = ctx.field(grid)
+    offset, size = seeds.seed_box(grid)
+    stride = np.float32(2)
+    parts = seeds.generate(offset, size, (grid.spacing * stride).astype(np.float32), 60)
+    adv = ParticleAdvector(ctx, len(parts), "none", "runge_kutta_4", 0.02, False, False)
+    out = adv.advect(field, parts).inactive_particles
+    got = dpa_b200.estimate_ftle(ctx, field, 60, (2, 2, 2), 0.02, out, mapping)
+    want, info = oracle.ftle(grid.shape, grid.offset, grid.spacing, (2, 2, 2), 60, 0.02,
+                             out.original_position, out.position, 0 if mapping == "reference" else 1)
+    assert got.data.shape == want.shape == (32, 32, 32)
+    finite = np.isfinite(want)
+    np.testing.assert_array_equal(np.isfinite(got.data), finite)
+    np.testing.assert_allclose(got.data[finite], want[finite], rtol=1e-3, atol=1e-6)
