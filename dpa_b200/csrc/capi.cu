@@ -12,100 +12,8 @@
 #include <string>
 #include <vector>
 
+#include "handles.cuh"
 #include "kernels.cuh"
-
-namespace {
-
-struct DeviceBuffer {
-  void* ptr = nullptr;
-  size_t bytes = 0;
-  cudaError_t reserve(size_t n) {
-    if (n <= bytes && ptr) return cudaSuccess;
-    release();
-    if (n == 0) n = 16;
-    cudaError_t e = cudaMalloc(&ptr, n);
-    if (e != cudaSuccess) {
-      ptr = nullptr;
-      return e;
-    }
-    bytes = n;
-    return cudaSuccess;
-  }
-  void release() {
-    if (ptr) cudaFree(ptr);
-    ptr = nullptr;
-    bytes = 0;
-  }
-  template <class T>
-  T* as() const { return static_cast<T*>(ptr); }
-};
-
-struct PinnedBuffer {
-  void* ptr = nullptr;
-  size_t bytes = 0;
-  cudaError_t reserve(size_t n) {
-    if (n <= bytes && ptr) return cudaSuccess;
-    release();
-    if (n == 0) n = 16;
-    cudaError_t e = cudaMallocHost(&ptr, n);
-    if (e != cudaSuccess) {
-      ptr = nullptr;
-      return e;
-    }
-    bytes = n;
-    return cudaSuccess;
-  }
-  void release() {
-    if (ptr) cudaFreeHost(ptr);
-    ptr = nullptr;
-    bytes = 0;
-  }
-  template <class T>
-  T* as() const { return static_cast<T*>(ptr); }
-};
-
-}  // namespace
-
-struct dpa_context {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  std::string error;
-  uint64_t staging_limit = 1ull << 30;
-
-  DeviceBuffer positions, remaining, remaining_in, termination;
-  DeviceBuffer keys, values, sort_temp;
-  uint64_t launches = 0;  // kernels this context launched (advection path)
-  bool profiling = false;
-  cudaEvent_t events[3] = {nullptr, nullptr, nullptr};  // order, advect begin, advect end
-  bool timed_order = false;
-  DeviceBuffer raw, raw_offsets, raw_counts, kept_vertices, kept_segments;
-  DeviceBuffer wide, vertex_offsets, segment_offsets, scan_temp, totals;
-  DeviceBuffer out_vertices, out_colors, out_indices;
-  PinnedBuffer host_vertices, host_colors, host_indices, host_totals;
-  DeviceBuffer ftle_winners, ftle_flow, ftle_out, ftle_original, ftle_final;
-
-  void release_all() {
-    DeviceBuffer* d[] = {&positions, &remaining, &remaining_in, &termination, &keys, &values,
-                         &sort_temp, &raw, &raw_offsets, &raw_counts,
-                         &kept_vertices, &kept_segments, &wide, &vertex_offsets,
-                         &segment_offsets, &scan_temp, &totals, &out_vertices, &out_colors,
-                         &out_indices, &ftle_winners, &ftle_flow, &ftle_out, &ftle_original,
-                         &ftle_final};
-    for (DeviceBuffer* b : d) b->release();
-    PinnedBuffer* h[] = {&host_vertices, &host_colors, &host_indices, &host_totals};
-    for (PinnedBuffer* b : h) b->release();
-  }
-};
-
-struct dpa_field {
-  dpa_context* owner = nullptr;
-  DeviceBuffer nodes;
-  dpa::FieldView view{};
-  uint64_t shape[3] = {0, 0, 0};
-  float offset[3] = {0, 0, 0};
-  float spacing[3] = {0, 0, 0};
-  int32_t storage = DPA_STORAGE_F32;
-};
 
 namespace {
 
