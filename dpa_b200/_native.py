@@ -40,6 +40,8 @@ TERMINATION = {0: "complete", 1: "out_of_bounds", 2: "zero_velocity"}
 
 FTLE_MAPPING = {"reference": 0, "lattice": 1}
 
+NO_ALLOC_MAX_PARTICLES = 1 << 20
+
 
 class AdvectOptions(C.Structure):
     _fields_ = [
@@ -93,6 +95,8 @@ SIGNATURES = {
     "dpa_advect_round": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _P, _P, _P,
                                    CURVE_SINK, _P]),
     "dpa_advect_device": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _P, _P, _P, _P]),
+    "dpa_advect_device_no_alloc": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _P, _P,
+                                             _P, _P]),
     "dpa_seed_lattice_device": (C.c_int, [_P, _F32P, _F32P, _F32P, _F32P, _U64P, _U64P, _P, _P]),
     "dpa_ftle_estimate": (C.c_int, [_P, _P, _F32P, C.c_uint64, C.c_float, C.c_uint64, _P, _P,
                                     C.c_int32, _P, _U64P]),

@@ -1,0 +1,126 @@
+// noalloc.cu -- dpa_advect_device_no_alloc: the device advection entry point
+// for callers that must not allocate device memory once they are running.
+//
+// Who needs it: a host program whose device memory is reserved up front by
+// another owner (a framework's caching allocator, or a service that fixes its
+// HBM budget at start-up) cannot count on a cudaMalloc succeeding later, and a
+// latency-bound loop cannot afford one: cudaMalloc and cudaFree may
+// synchronize the whole device and so stall work queued on other streams.
+// dpa_advect_device grows its ordering scratch with cudaMalloc; this variant
+// takes it from a fixed array compiled into the library instead.
+//
+// The array below is a file-scope __device__ array of kScratchBytes (about
+// 6.3 MiB). Every GPU on which the library's code is loaded holds its own copy
+// until the process exits. Host code cannot use the name g_scratch as a device
+// address (on the host it names a host-side stand-in), so the device address
+// is looked up once per device with cudaGetSymbolAddress, with that device
+// current, and handed to the kernels.
+#include <mutex>
+
+#include "handles.cuh"
+#include "kernels.cuh"
+
+namespace {
+
+constexpr uint64_t kMaxParticles = DPA_NO_ALLOC_MAX_PARTICLES;
+constexpr size_t kAlign = 256;
+constexpr size_t round_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
+
+// Scratch layout: bucket counters, then the processing order, then the
+// per-particle bucket ids.
+constexpr size_t kCountsOffset = 0;
+constexpr size_t kOrderOffset = round_up(size_t(dpa::kOrderBuckets + 1) * sizeof(uint32_t));
+constexpr size_t kBucketsOffset = kOrderOffset + round_up(kMaxParticles * sizeof(uint32_t));
+constexpr size_t kScratchBytes = kBucketsOffset + round_up(kMaxParticles * sizeof(uint16_t));
+
+static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_lock;
+void* g_device_address[kMaxDevices] = {};
+
+// Device address of g_scratch on `device`, which must be current. The first
+// call per device resolves it (and, with lazy module loading, loads this
+// file's module on that device); later calls return the cached address.
+cudaError_t scratch_on(int device, unsigned char** out) {
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> guard(g_lock);
+  if (!g_device_address[device]) {
+    void* address = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&address, g_scratch);
+    if (e != cudaSuccess) return e;
+    g_device_address[device] = address;
+  }
+  *out = static_cast<unsigned char*>(g_device_address[device]);
+  return cudaSuccess;
+}
+
+int refuse(dpa_context* ctx, int status, const char* message) {
+  ctx->error = message;
+  return status;
+}
+
+int refuse_cuda(dpa_context* ctx, cudaError_t e, const char* where) {
+  ctx->error = std::string(where) + ": " + cudaGetErrorName(e);
+  return DPA_ERROR_CUDA;
+}
+
+}  // namespace
+
+extern "C" int dpa_advect_device_no_alloc(dpa_context* ctx, const dpa_field* field,
+                                          const dpa_advect_options* options, uint64_t count,
+                                          float* device_positions, uint64_t* device_remaining,
+                                          uint8_t* device_termination, void* stream) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  try {
+    if (!options) return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT, "options is NULL");
+    if (!field || field->owner != ctx) return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT, "bad field");
+    if (options->record)
+      return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT,
+                    "dpa_advect_device_no_alloc does not record; use dpa_advect_round");
+    if (options->integrator != DPA_INTEGRATOR_EULER &&
+        options->integrator != DPA_INTEGRATOR_RUNGE_KUTTA_4 &&
+        options->integrator != DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE)
+      return refuse(ctx, DPA_ERROR_UNSUPPORTED,
+                    "integrator not implemented on the GPU (euler, runge_kutta_4 and "
+                    "runge_kutta_4_true are)");
+    if (count > kMaxParticles)
+      return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT,
+                    "dpa_advect_device_no_alloc: count exceeds DPA_NO_ALLOC_MAX_PARTICLES "
+                    "(1048576); split the particles or use dpa_advect_device");
+    if (count && (!device_positions || !device_remaining))
+      return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT, "positions or remaining is NULL");
+    if (count == 0) return DPA_OK;
+
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return refuse_cuda(ctx, e, "cudaSetDevice");
+    unsigned char* scratch = nullptr;
+    e = scratch_on(ctx->device, &scratch);
+    if (e != cudaSuccess) return refuse_cuda(ctx, e, "cudaGetSymbolAddress");
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
+
+    const uint32_t* order = nullptr;
+    if (options->morton_order && count >= 2) {
+      // launch_order starts by zeroing the counters, so what an earlier call
+      // left in the shared array does not matter.
+      uint32_t* counts = reinterpret_cast<uint32_t*>(scratch + kCountsOffset);
+      uint32_t* order_out = reinterpret_cast<uint32_t*>(scratch + kOrderOffset);
+      uint16_t* buckets = reinterpret_cast<uint16_t*>(scratch + kBucketsOffset);
+      e = dpa::launch_order(field->view, device_positions, count, buckets, counts, order_out, s);
+      if (e != cudaSuccess) return refuse_cuda(ctx, e, "ordering kernels");
+      order = order_out;
+    }
+    dpa::AdvectArgs a{};
+    a.count = count;
+    a.order = order;
+    a.positions = device_positions;
+    a.remaining = device_remaining;
+    a.termination = device_termination;
+    a.coefficients = dpa::make_step_coefficients(options->step_size);
+    e = dpa::launch_advect(field->view, a, options->integrator, false, s);
+    if (e != cudaSuccess) return refuse_cuda(ctx, e, "advection kernel");
+    return DPA_OK;
+  } catch (...) {
+    return DPA_ERROR_INTERNAL;
+  }
+}

@@ -191,6 +191,31 @@ int dpa_advect_device(dpa_context* ctx, const dpa_field* field, const dpa_advect
                       uint64_t count, float* device_positions, uint64_t* device_remaining,
                       uint8_t* device_termination, void* stream);
 
+/* ---- allocation-free advection ----------------------------------------------- */
+
+/* No counterpart in the reference. dpa_advect_device for callers that must not
+ * allocate device memory while running: programs whose device memory is
+ * reserved up front by another owner (a framework's caching allocator, a
+ * service with a fixed HBM budget), and latency-bound loops, since cudaMalloc
+ * and cudaFree may synchronize the whole device and stall other streams.
+ * Same inputs, outputs and results as dpa_advect_device (recording is not
+ * offered); the ordering scratch comes from a fixed device array inside the
+ * library (about 6.3 MiB, held by every GPU on which the library's code is
+ * loaded until the process exits) instead of cudaMalloc. At most
+ * DPA_NO_ALLOC_MAX_PARTICLES particles per call; more is rejected with
+ * DPA_ERROR_INVALID_ARGUMENT. The first call on a device resolves the array's
+ * device address (and may load the library's code on that device), so make
+ * it during set-up, before any stream capture. Every call shares the one
+ * array: calls whose work overlaps on the GPU (two streams, or two contexts
+ * on one device) race; order them on one stream or synchronize between
+ * them. Asynchronous like dpa_advect_device. */
+#define DPA_NO_ALLOC_MAX_PARTICLES 1048576u
+
+int dpa_advect_device_no_alloc(dpa_context* ctx, const dpa_field* field,
+                               const dpa_advect_options* options, uint64_t count,
+                               float* device_positions, uint64_t* device_remaining,
+                               uint8_t* device_termination, void* stream);
+
 /* ---- seeds ------------------------------------------------------------------- */
 
 /* Lattice seeds on the device: uniform_seed_generator::generate
