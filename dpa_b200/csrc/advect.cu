@@ -27,62 +27,128 @@ struct CurveCounter {
   }
 };
 
+// Persistent advection: every lane owns one particle at a time and, when it
+// finishes, takes the next one from its warp's claim of kClaim consecutive
+// entries of the processing order; the warp claims a new batch with one
+// atomic when its batch runs out. Lanes therefore stay busy while particles
+// of one warp end after very different numbers of steps.
 template <int kIntegrator, int kStorage, bool kPow2, bool kRecord>
-__global__ void __launch_bounds__(kAdvectBlock)
+__global__ void __launch_bounds__(kAdvectBlock, kAdvectMinBlocks)
 advect_kernel(const FieldView f, const AdvectArgs a) {
-  const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= a.count) return;
-  const uint64_t k = a.order ? a.order[t] : t;
+  constexpr unsigned kFull = 0xffffffffu;
+  constexpr uint32_t kClaim = 32;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lanes_below = (1u << lane) - 1u;
 
-  float p[3] = {a.positions[3 * k], a.positions[3 * k + 1], a.positions[3 * k + 2]};
-  const uint64_t remaining = a.remaining[k];
+  // Warp-uniform claim: entries [claim_next, claim_end) of the order.
+  uint64_t claim_next = 0, claim_end = 0;
+  bool exhausted = false;
 
+  bool active = false;
+  uint64_t k = 0, remaining = 0, it = 0;
+  Position p{0.0f, make_float2(0.0f, 0.0f)};
   float* curve = nullptr;
   CurveCounter counter;
-  if constexpr (kRecord) {
-    curve = a.raw_vertices + 3 * a.raw_offsets[k];
-    curve[0] = p[0];
-    curve[1] = p[1];
-    curve[2] = p[2];
-    counter.append(p[0], p[1], p[2]);
-  }
-
   CellSampler<kStorage, kPow2> sampler;
-  uint64_t it = 0;
-  int reason = DPA_TERMINATION_COMPLETE;
-  for (; it < remaining; ++it) {
-    const int r = step<kIntegrator, kStorage, kPow2>(f, a.coefficients, sampler, p);
-    if (r != kStepTaken) {
-      reason = r == kStepOutOfBounds ? DPA_TERMINATION_OUT_OF_BOUNDS : DPA_TERMINATION_ZERO_VELOCITY;
-      break;
+
+  while (true) {
+    // Hand new particles to idle lanes.
+    unsigned idle = __ballot_sync(kFull, !active);
+    while (idle && !exhausted) {
+      if (claim_next == claim_end) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(a.work_counter, (unsigned long long)kClaim);
+        base = __shfl_sync(kFull, base, 0);
+        if (base >= a.count) {
+          exhausted = true;
+          break;
+        }
+        claim_next = base;
+        claim_end = base + kClaim < a.count ? base + kClaim : a.count;
+      }
+      const uint32_t left = uint32_t(claim_end - claim_next);
+      const uint32_t take = uint32_t(__popc(idle)) < left ? uint32_t(__popc(idle)) : left;
+      const uint32_t rank = __popc(idle & lanes_below);
+      const bool mine = !active && rank < take;
+      if (mine) {
+        const uint64_t t = claim_next + rank;
+        k = a.order ? a.order[t] : t;
+        p.p0 = a.positions[3 * k];
+        p.p21 = make_float2(a.positions[3 * k + 2], a.positions[3 * k + 1]);
+        remaining = a.remaining[k];
+        it = 0;
+        sampler.reset();
+        active = true;
+        if constexpr (kRecord) {
+          curve = a.raw_vertices + 3 * a.raw_offsets[k];
+          curve[0] = p.p0;
+          curve[1] = p.p21.y;
+          curve[2] = p.p21.x;
+          counter = CurveCounter();
+          counter.append(p.p0, p.p21.y, p.p21.x);
+        }
+      }
+      claim_next += take;
+      idle &= ~__ballot_sync(kFull, mine);
     }
-    if constexpr (kRecord) {
-      float* v = curve + 3 * (it + 1);
-      v[0] = p[0];
-      v[1] = p[1];
-      v[2] = p[2];
-      counter.append(p[0], p[1], p[2]);
+    if (!__any_sync(kFull, active)) break;
+
+    if (active) {
+      int r = kStepTaken;
+      if (it < remaining) {
+        r = step<kIntegrator, kStorage, kPow2>(f, a.coefficients, sampler, p);
+        if (r == kStepTaken) {
+          ++it;
+          if constexpr (kRecord) {
+            float* v = curve + 3 * it;
+            v[0] = p.p0;
+            v[1] = p.p21.y;
+            v[2] = p.p21.x;
+            counter.append(p.p0, p.p21.y, p.p21.x);
+          }
+        }
+      }
+      if (r != kStepTaken || it >= remaining) {
+        const int reason = r == kStepTaken        ? DPA_TERMINATION_COMPLETE
+                           : r == kStepOutOfBounds ? DPA_TERMINATION_OUT_OF_BOUNDS
+                                                   : DPA_TERMINATION_ZERO_VELOCITY;
+        if constexpr (kRecord) {
+          float* v = curve + 3 * (it + 1);
+          v[0] = kTerminal;
+          v[1] = kTerminal;
+          v[2] = kTerminal;
+          counter.append(kTerminal, kTerminal, kTerminal);
+          a.kept_vertices[k] = counter.kept;
+          a.kept_segments[k] = counter.segments;
+        }
+        a.positions[3 * k] = p.p0;
+        a.positions[3 * k + 1] = p.p21.y;
+        a.positions[3 * k + 2] = p.p21.x;
+        a.remaining[k] = remaining - it;
+        if (a.termination) a.termination[k] = uint8_t(reason);
+        active = false;
+      }
     }
   }
-  if constexpr (kRecord) {
-    float* v = curve + 3 * (it + 1);
-    v[0] = kTerminal;
-    v[1] = kTerminal;
-    v[2] = kTerminal;
-    counter.append(kTerminal, kTerminal, kTerminal);
-    a.kept_vertices[k] = counter.kept;
-    a.kept_segments[k] = counter.segments;
-  }
-  a.positions[3 * k] = p[0];
-  a.positions[3 * k + 1] = p[1];
-  a.positions[3 * k + 2] = p[2];
-  a.remaining[k] = remaining - it;
-  if (a.termination) a.termination[k] = uint8_t(reason);
 }
 
 template <int kIntegrator, int kStorage, bool kPow2, bool kRecord>
 cudaError_t launch_typed(const FieldView& f, const AdvectArgs& a, cudaStream_t stream) {
-  const uint64_t blocks = (a.count + kAdvectBlock - 1) / kAdvectBlock;
+  // Persistent grid: as many blocks as fit on the device at once, fewer when
+  // there are fewer particles than lanes.
+  static int resident = 0;  // blocks per SM, per instantiation
+  static int sms = 0;
+  if (resident == 0) {
+    int device = 0;
+    DPA_CUDA_TRY(cudaGetDevice(&device));
+    DPA_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    DPA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &resident, advect_kernel<kIntegrator, kStorage, kPow2, kRecord>, kAdvectBlock, 0));
+    if (resident < 1) resident = 1;
+  }
+  const uint64_t needed = (a.count + kAdvectBlock - 1) / kAdvectBlock;
+  const uint64_t blocks = std::min<uint64_t>(needed, uint64_t(resident) * uint64_t(sms));
+  DPA_CUDA_TRY(cudaMemsetAsync(a.work_counter, 0, sizeof(unsigned long long), stream));
   advect_kernel<kIntegrator, kStorage, kPow2, kRecord>
       <<<dim3(unsigned(blocks)), dim3(kAdvectBlock), 0, stream>>>(f, a);
   return cudaGetLastError();
@@ -124,9 +190,8 @@ __device__ __forceinline__ uint32_t order_bucket(const FieldView& f, const float
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     const float q = (p[i] - f.offset[i]) * (1.0f / f.spacing[i]);
-    const float s = floorf(q);
-    if (!(s >= 0.0f && s <= f.limit[i])) return kOrderBuckets;
-    c[i] = uint32_t(s) * 16u / uint32_t(f.n[i]);
+    if (!(q >= 0.0f && q < f.upper[i])) return kOrderBuckets;
+    c[i] = uint32_t(floorf(q)) * 16u / uint32_t(f.n[i]);
   }
   return (spread4(c[0]) << 2) | (spread4(c[1]) << 1) | spread4(c[2]);
 }

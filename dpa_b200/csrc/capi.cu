@@ -113,7 +113,9 @@ int advect_device_impl(dpa_context* ctx, const dpa_field* field, const dpa_advec
     if (st != DPA_OK) return st;
   }
   if (ctx->profiling) DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->events[1], s));
+  DPA_TRY_CUDA(ctx, ctx->work_counter.reserve(sizeof(unsigned long long)));
   dpa::AdvectArgs a{};
+  a.work_counter = ctx->work_counter.as<unsigned long long>();
   a.count = count;
   a.order = order;
   a.positions = positions;
@@ -175,7 +177,9 @@ int record_piece(dpa_context* ctx, const dpa_field* field, const dpa_advect_opti
     const int st = build_order(ctx, field, positions, n, s, &order);
     if (st != DPA_OK) return st;
   }
+  DPA_TRY_CUDA(ctx, ctx->work_counter.reserve(sizeof(unsigned long long)));
   dpa::AdvectArgs a{};
+  a.work_counter = ctx->work_counter.as<unsigned long long>();
   a.count = n;
   a.order = order;
   a.positions = positions;
@@ -448,7 +452,7 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
       v.offset[i] = offset[i];
       v.spacing[i] = spacing[i];
       v.inv_spacing[i] = 1.0f / spacing[i];
-      v.limit[i] = float(int64_t(shape[i]) - 2);
+      v.upper[i] = float(int64_t(shape[i]) - 1);
     }
     v.stride0 = int64_t(shape[1]) * int64_t(shape[2]);
     v.stride1 = int32_t(shape[2]);

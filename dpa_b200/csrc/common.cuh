@@ -33,7 +33,7 @@ struct FieldView {
   float offset[3];
   float spacing[3];
   float inv_spacing[3];  // exact reciprocals, used only when pow2 is set
-  float limit[3];        // n - 2: largest valid cell subscript
+  float upper[3];        // n - 1: inside iff 0 <= (p - offset) / h < n - 1
   int32_t storage;       // dpa_storage
   int32_t pow2;          // every spacing is a power of two (division == product)
 };

@@ -68,7 +68,7 @@ struct dpa_context {
   uint64_t staging_limit = 1ull << 30;
 
   DeviceBuffer positions, remaining, remaining_in, termination;
-  DeviceBuffer keys, values, sort_temp;
+  DeviceBuffer keys, values, sort_temp, work_counter;
   uint64_t launches = 0;  // kernels this context launched (advection path)
   bool profiling = false;
   cudaEvent_t events[3] = {nullptr, nullptr, nullptr};  // order, advect begin, advect end
@@ -81,7 +81,7 @@ struct dpa_context {
 
   void release_all() {
     DeviceBuffer* d[] = {&positions, &remaining, &remaining_in, &termination, &keys, &values,
-                         &sort_temp, &raw, &raw_offsets, &raw_counts,
+                         &sort_temp, &work_counter, &raw, &raw_offsets, &raw_counts,
                          &kept_vertices, &kept_segments, &wide, &vertex_offsets,
                          &segment_offsets, &scan_temp, &totals, &out_vertices, &out_colors,
                          &out_indices, &ftle_winners, &ftle_flow, &ftle_out, &ftle_original,

@@ -6,6 +6,10 @@
 namespace dpa {
 
 constexpr int kAdvectBlock = 256;
+#ifndef DPA_ADVECT_MIN_BLOCKS
+#define DPA_ADVECT_MIN_BLOCKS 4
+#endif
+constexpr int kAdvectMinBlocks = DPA_ADVECT_MIN_BLOCKS;
 
 struct AdvectArgs {
   uint64_t count;
@@ -14,6 +18,7 @@ struct AdvectArgs {
   uint64_t* remaining;    // [count], updated in place
   uint8_t* termination;   // [count] or null
   StepCoefficients coefficients;
+  unsigned long long* work_counter;  // zeroed by the launcher; claims of the order
   // Recording only.
   float* raw_vertices;          // unpruned curve of particle k at raw_offsets[k]
   const uint64_t* raw_offsets;  // exclusive scan of remaining + 2

@@ -26,10 +26,12 @@ constexpr uint64_t kMaxParticles = DPA_NO_ALLOC_MAX_PARTICLES;
 constexpr size_t kAlign = 256;
 constexpr size_t round_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign; }
 
-// Scratch layout: bucket counters, then the processing order, then the
-// per-particle bucket ids.
-constexpr size_t kCountsOffset = 0;
-constexpr size_t kOrderOffset = round_up(size_t(dpa::kOrderBuckets + 1) * sizeof(uint32_t));
+// Scratch layout: the advection kernel's work counter, the bucket counters,
+// the processing order, the per-particle bucket ids.
+constexpr size_t kCounterOffset = 0;
+constexpr size_t kCountsOffset = kAlign;
+constexpr size_t kOrderOffset =
+    kCountsOffset + round_up(size_t(dpa::kOrderBuckets + 1) * sizeof(uint32_t));
 constexpr size_t kBucketsOffset = kOrderOffset + round_up(kMaxParticles * sizeof(uint32_t));
 constexpr size_t kScratchBytes = kBucketsOffset + round_up(kMaxParticles * sizeof(uint16_t));
 
@@ -111,6 +113,8 @@ extern "C" int dpa_advect_device_no_alloc(dpa_context* ctx, const dpa_field* fie
       order = order_out;
     }
     dpa::AdvectArgs a{};
+    // launch_advect zeroes the work counter before the kernel starts.
+    a.work_counter = reinterpret_cast<unsigned long long*>(scratch + kCounterOffset);
     a.count = count;
     a.order = order;
     a.positions = device_positions;

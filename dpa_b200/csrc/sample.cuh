@@ -35,80 +35,144 @@ __device__ __forceinline__ void load_node(const void* nodes, int64_t index, floa
   }
 }
 
-// Where a position falls in the grid: a = p - offset, s = floor(a / h).
-// Inside iff 0 <= s <= n - 2 on every axis (NaN is outside), which is
-// regular_grid::contains.
-template <bool kPow2>
-__device__ __forceinline__ bool locate(const FieldView& f, const float p[3], float a[3],
-                                       float s[3]) {
-  bool inside = true;
-#pragma unroll
-  for (int i = 0; i < 3; ++i) {
-    a[i] = __fsub_rn(p[i], f.offset[i]);
-    const float q = kPow2 ? __fmul_rn(a[i], f.inv_spacing[i]) : __fdiv_rn(a[i], f.spacing[i]);
-    s[i] = floorf(q);
-    inside = inside && (s[i] >= 0.0f) && (s[i] <= f.limit[i]);
-  }
-  return inside;
+// Two FP32 lanes, each rounded on its own with the scalar __fadd_rn /
+// __fmul_rn, which the compiler never contracts into an FMA. (sm_100's packed
+// f32x2 add and multiply are contracted into packed FMAs by the compiler even
+// with explicit .rn rounding, so they cannot reproduce the reference's
+// separately rounded products and sums.)
+__device__ __forceinline__ float2 add2(float2 a, float2 b) {
+  return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
 }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+  return make_float2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
+}
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 splat(float a) { return make_float2(a, a); }
 
-// fmod(a, h) / h for 0 <= a, given s = floor(fl(a / h)). The rounded quotient
-// is either the true integer quotient N or N + 1 (only when a / h lies within
-// half an ulp below N + 1, so fmod(a, h) >= h / 2). In both cases a - s * h is
-// exactly representable, so one FMA gives it exactly; adding h back in the
-// N + 1 case is exact too. fmod keeps the dividend's sign for a zero result.
-template <bool kPow2>
-__device__ __forceinline__ float weight(float a, float s, float h, float inv_h) {
+// A particle position is held as p0 and the pair p21 = (p2, p1): the
+// derivative of (p2, p1) is (v0, v1), the first two components of a sample,
+// because of the reversed components of particle_advector.cpp:369.
+struct Position {
+  float p0;
+  float2 p21;
+};
+
+// Weights of one sample: w = fmod(p - offset, h) / h per axis, as (w0, (w2, w1)).
+struct Weights {
+  float w0;
+  float2 w21;
+};
+
+// Where a position falls in the grid, per axis: the rounded quotient
+// q = (p - offset) / h, its floor s (the cell subscript) and the weight
+// w = fmod(p - offset, h) / h, all as the reference rounds them. The position
+// is inside iff 0 <= s <= n - 2 on every axis (regular_grid::contains), which
+// for any float q (NaN included) is 0 <= q < n - 1.
+//
+// Power-of-two spacing: a / h is exact, and so is fmod(a, h) / h = q - s, whose
+// difference is representable; the sign of a zero weight follows q as fmod's
+// follows a.
+//
+// Other spacings: the rounded quotient is either the true integer quotient N
+// or N + 1 (only when a / h lies within half an ulp below N + 1, so that
+// fmod(a, h) >= h / 2). In both cases a - s * h is exactly representable, so
+// one FMA gives it exactly; adding h back in the N + 1 case is exact too.
+__device__ __forceinline__ float weight_general(float a, float s, float h) {
   float r = fmaf(-s, h, a);
   if (r < 0.0f) r = __fadd_rn(r, h);
   if (r == 0.0f) r = copysignf(0.0f, a);
-  return kPow2 ? __fmul_rn(r, inv_h) : __fdiv_rn(r, h);
+  return __fdiv_rn(r, h);
 }
 
-// (1 - w) * lo + w * hi with every operation rounded on its own.
-__device__ __forceinline__ float lerp_ref(float lo, float hi, float one_minus_w, float w) {
-  return __fadd_rn(__fmul_rn(one_minus_w, lo), __fmul_rn(w, hi));
+template <bool kPow2>
+__device__ __forceinline__ bool locate(const FieldView& f, const Position& p, int cell[3],
+                                       Weights& w) {
+  const float a0 = __fsub_rn(p.p0, f.offset[0]);
+  const float2 a21 = add2(p.p21, neg2(make_float2(f.offset[2], f.offset[1])));
+  float q0, q2, q1;
+  if constexpr (kPow2) {
+    q0 = __fmul_rn(a0, f.inv_spacing[0]);
+    const float2 q21 = mul2(a21, make_float2(f.inv_spacing[2], f.inv_spacing[1]));
+    q2 = q21.x;
+    q1 = q21.y;
+  } else {
+    q0 = __fdiv_rn(a0, f.spacing[0]);
+    q2 = __fdiv_rn(a21.x, f.spacing[2]);
+    q1 = __fdiv_rn(a21.y, f.spacing[1]);
+  }
+  const bool inside = (q0 >= 0.0f) && (q0 < f.upper[0]) && (q1 >= 0.0f) && (q1 < f.upper[1]) &&
+                      (q2 >= 0.0f) && (q2 < f.upper[2]);
+  const float s0 = floorf(q0), s1 = floorf(q1), s2 = floorf(q2);
+  if constexpr (kPow2) {
+    w.w0 = copysignf(__fsub_rn(q0, s0), q0);
+    const float2 d = add2(make_float2(q2, q1), neg2(make_float2(s2, s1)));
+    w.w21 = make_float2(copysignf(d.x, q2), copysignf(d.y, q1));
+  } else {
+    w.w0 = weight_general(a0, s0, f.spacing[0]);
+    w.w21 = make_float2(weight_general(a21.x, s2, f.spacing[2]),
+                        weight_general(a21.y, s1, f.spacing[1]));
+  }
+  cell[0] = int(s0);
+  cell[1] = int(s1);
+  cell[2] = int(s2);
+  return inside;
 }
 
-// The eight corners of one cell: corner[dx * 4 + dy * 2 + dz][component].
+// The eight corners of one cell, corner j = dx * 4 + dy * 2 + dz (the
+// permute_for order of permute_for.hpp:12-34), arranged for packed lerps:
+// xy[j] = (v0, v1) of corner j, and the v2 components paired as
+// (corner 0, corner 4), (1, 5), (2, 6), (3, 7).
 struct Corners {
-  float c[8][3];
+  float2 xy[8];
+  float2 z04, z15, z26, z37;
 };
 
 template <int kStorage>
-__device__ __forceinline__ void gather(const FieldView& f, int i0, int i1, int i2, Corners& k) {
-  const int64_t base = int64_t(i0) * f.stride0 + int64_t(i1) * f.stride1 + i2;
+__device__ __forceinline__ void gather(const FieldView& f, const int cell[3], Corners& k) {
+  const int64_t base = int64_t(cell[0]) * f.stride0 + int64_t(cell[1]) * f.stride1 + cell[2];
   const int64_t s0 = f.stride0, s1 = f.stride1;
-  load_node<kStorage>(f.nodes, base, k.c[0][0], k.c[0][1], k.c[0][2]);
-  load_node<kStorage>(f.nodes, base + 1, k.c[1][0], k.c[1][1], k.c[1][2]);
-  load_node<kStorage>(f.nodes, base + s1, k.c[2][0], k.c[2][1], k.c[2][2]);
-  load_node<kStorage>(f.nodes, base + s1 + 1, k.c[3][0], k.c[3][1], k.c[3][2]);
-  load_node<kStorage>(f.nodes, base + s0, k.c[4][0], k.c[4][1], k.c[4][2]);
-  load_node<kStorage>(f.nodes, base + s0 + 1, k.c[5][0], k.c[5][1], k.c[5][2]);
-  load_node<kStorage>(f.nodes, base + s0 + s1, k.c[6][0], k.c[6][1], k.c[6][2]);
-  load_node<kStorage>(f.nodes, base + s0 + s1 + 1, k.c[7][0], k.c[7][1], k.c[7][2]);
+  float z[8];
+  load_node<kStorage>(f.nodes, base, k.xy[0].x, k.xy[0].y, z[0]);
+  load_node<kStorage>(f.nodes, base + 1, k.xy[1].x, k.xy[1].y, z[1]);
+  load_node<kStorage>(f.nodes, base + s1, k.xy[2].x, k.xy[2].y, z[2]);
+  load_node<kStorage>(f.nodes, base + s1 + 1, k.xy[3].x, k.xy[3].y, z[3]);
+  load_node<kStorage>(f.nodes, base + s0, k.xy[4].x, k.xy[4].y, z[4]);
+  load_node<kStorage>(f.nodes, base + s0 + 1, k.xy[5].x, k.xy[5].y, z[5]);
+  load_node<kStorage>(f.nodes, base + s0 + s1, k.xy[6].x, k.xy[6].y, z[6]);
+  load_node<kStorage>(f.nodes, base + s0 + s1 + 1, k.xy[7].x, k.xy[7].y, z[7]);
+  k.z04 = make_float2(z[0], z[4]);
+  k.z15 = make_float2(z[1], z[5]);
+  k.z26 = make_float2(z[2], z[6]);
+  k.z37 = make_float2(z[3], z[7]);
 }
 
-// Reduce axis 2, then 1, then 0 (regular_grid.hpp:71-73).
-__device__ __forceinline__ void trilinear(const Corners& k, const float w[3], float v[3]) {
-  const float tz = __fsub_rn(1.0f, w[2]);
-  const float ty = __fsub_rn(1.0f, w[1]);
-  const float tx = __fsub_rn(1.0f, w[0]);
-#pragma unroll
-  for (int c = 0; c < 3; ++c) {
-    const float e0 = lerp_ref(k.c[0][c], k.c[1][c], tz, w[2]);
-    const float e1 = lerp_ref(k.c[2][c], k.c[3][c], tz, w[2]);
-    const float e2 = lerp_ref(k.c[4][c], k.c[5][c], tz, w[2]);
-    const float e3 = lerp_ref(k.c[6][c], k.c[7][c], tz, w[2]);
-    const float f0 = lerp_ref(e0, e1, ty, w[1]);
-    const float f1 = lerp_ref(e2, e3, ty, w[1]);
-    v[c] = lerp_ref(f0, f1, tx, w[0]);
-  }
+// (1 - w) * lo + w * hi per lane, every operation rounded on its own.
+__device__ __forceinline__ float2 lerp2(float2 lo, float2 hi, float2 one_minus_w, float2 w) {
+  return add2(mul2(one_minus_w, lo), mul2(w, hi));
 }
 
-__device__ __forceinline__ bool is_zero(const float v[3]) {
-  return fabsf(v[0]) <= kZeroPrecision && fabsf(v[1]) <= kZeroPrecision &&
-         fabsf(v[2]) <= kZeroPrecision;
+// Trilinear reduction of regular_grid.hpp:71-73: axis 2, then 1, then 0, with
+// c[j] = (1 - w) * c[2j] + w * c[2j+1]. Components 0 and 1 travel as one pair;
+// component 2 pairs the reductions of the x0 and x1 halves of the cell.
+__device__ __forceinline__ void trilinear(const Corners& k, const Weights& w, float2& v01,
+                                          float& v2) {
+  const float2 one = splat(1.0f);
+  const float2 t21 = add2(one, neg2(w.w21));
+  const float t0 = __fsub_rn(1.0f, w.w0);
+  const float2 W2 = splat(w.w21.x), T2 = splat(t21.x);
+  const float2 W1 = splat(w.w21.y), T1 = splat(t21.y);
+  const float2 W0 = splat(w.w0), T0 = splat(t0);
+  const float2 e0 = lerp2(k.xy[0], k.xy[1], T2, W2);
+  const float2 e1 = lerp2(k.xy[2], k.xy[3], T2, W2);
+  const float2 e2 = lerp2(k.xy[4], k.xy[5], T2, W2);
+  const float2 e3 = lerp2(k.xy[6], k.xy[7], T2, W2);
+  const float2 f0 = lerp2(e0, e1, T1, W1);
+  const float2 f1 = lerp2(e2, e3, T1, W1);
+  v01 = lerp2(f0, f1, T0, W0);
+  const float2 e02 = lerp2(k.z04, k.z15, T2, W2);  // (e0, e2) of component 2
+  const float2 e13 = lerp2(k.z26, k.z37, T2, W2);  // (e1, e3)
+  const float2 f01 = lerp2(e02, e13, T1, W1);      // (f0, f1)
+  v2 = __fadd_rn(__fmul_rn(t0, f01.x), __fmul_rn(w.w0, f01.y));
 }
 
 // A per-thread cache of the current cell's corners: a particle usually stays
@@ -117,75 +181,77 @@ __device__ __forceinline__ bool is_zero(const float v[3]) {
 template <int kStorage, bool kPow2>
 struct CellSampler {
   Corners corners;
-  int cell[3] = {-1, -1, -1};
+  int cached[3] = {-1, -1, -1};
 
-  // Samples at p; returns false when p is outside the grid.
-  __device__ __forceinline__ bool sample(const FieldView& f, const float p[3], float v[3]) {
-    float a[3], s[3];
-    if (!locate<kPow2>(f, p, a, s)) return false;
-    const int i0 = int(s[0]), i1 = int(s[1]), i2 = int(s[2]);
-    if (i0 != cell[0] || i1 != cell[1] || i2 != cell[2]) {
-      gather<kStorage>(f, i0, i1, i2, corners);
-      cell[0] = i0;
-      cell[1] = i1;
-      cell[2] = i2;
+  // Samples at p; returns false when p is outside the grid. The sample is
+  // returned as v01 = (v0, v1) and v2.
+  __device__ __forceinline__ bool sample(const FieldView& f, const Position& p, float2& v01,
+                                         float& v2) {
+    int cell[3];
+    Weights w;
+    if (!locate<kPow2>(f, p, cell, w)) return false;
+    if (cell[0] != cached[0] || cell[1] != cached[1] || cell[2] != cached[2]) {
+      gather<kStorage>(f, cell, corners);
+      cached[0] = cell[0];
+      cached[1] = cell[1];
+      cached[2] = cell[2];
     }
-    float w[3];
-#pragma unroll
-    for (int i = 0; i < 3; ++i) w[i] = weight<kPow2>(a[i], s[i], f.spacing[i], f.inv_spacing[i]);
-    trilinear(corners, w, v);
+    trilinear(corners, w, v01, v2);
     return true;
   }
+
+  __device__ __forceinline__ void reset() { cached[0] = cached[1] = cached[2] = -1; }
 };
+
+__device__ __forceinline__ bool is_zero(float2 v01, float v2) {
+  return fabsf(v01.x) <= kZeroPrecision && fabsf(v01.y) <= kZeroPrecision &&
+         fabsf(v2) <= kZeroPrecision;
+}
 
 enum StepResult : int { kStepTaken = 0, kStepOutOfBounds = 1, kStepZeroVelocity = 2 };
 
-// One integrator step in place. The derivative is the sample with reversed
-// components (particle_advector.cpp:369).
+// One integrator step in place. The derivative of p0 is v2 and that of
+// (p2, p1) is (v0, v1) (particle_advector.cpp:369).
 template <int kIntegrator, int kStorage, bool kPow2>
 __device__ __forceinline__ int step(const FieldView& f, const StepCoefficients& k,
-                                   CellSampler<kStorage, kPow2>& sampler, float p[3]) {
-  float v[3];
-  if (!sampler.sample(f, p, v)) return kStepOutOfBounds;
-  if (is_zero(v)) return kStepZeroVelocity;
-  const float d[3] = {v[2], v[1], v[0]};
+                                   CellSampler<kStorage, kPow2>& sampler, Position& p) {
+  float2 v01;
+  float v2;
+  if (!sampler.sample(f, p, v01, v2)) return kStepOutOfBounds;
+  if (is_zero(v01, v2)) return kStepZeroVelocity;
   if constexpr (kIntegrator == DPA_INTEGRATOR_EULER) {
     // odeint euler: x = 1 * x + dt * dxdt
-#pragma unroll
-    for (int c = 0; c < 3; ++c) p[c] = __fadd_rn(p[c], __fmul_rn(k.dt, d[c]));
+    p.p0 = __fadd_rn(p.p0, __fmul_rn(k.dt, v2));
+    p.p21 = add2(p.p21, mul2(splat(k.dt), v01));
   } else if constexpr (kIntegrator == DPA_INTEGRATOR_RUNGE_KUTTA_4) {
     // odeint runge_kutta4, final stage with four equal stage derivatives:
     // x = 1 * x + (b0 dt) d + (b1 dt) d + (b2 dt) d + (b3 dt) d, left to right.
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float m0 = __fmul_rn(k.c0, d[c]);
-      const float m1 = __fmul_rn(k.c1, d[c]);
-      p[c] = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(p[c], m0), m1), m1), m0);
-    }
+    const float m0 = __fmul_rn(k.c0, v2), m1 = __fmul_rn(k.c1, v2);
+    p.p0 = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(p.p0, m0), m1), m1), m0);
+    const float2 n0 = mul2(splat(k.c0), v01), n1 = mul2(splat(k.c1), v01);
+    p.p21 = add2(add2(add2(add2(p.p21, n0), n1), n1), n0);
   } else {
     // Four-sample RK4; a stage outside the grid ends the particle without
     // taking the step.
-    float x[3], k2[3], k3[3], k4[3], w[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) x[c] = __fadd_rn(p[c], __fmul_rn(k.half, d[c]));
-    if (!sampler.sample(f, x, w)) return kStepOutOfBounds;
-    k2[0] = w[2]; k2[1] = w[1]; k2[2] = w[0];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) x[c] = __fadd_rn(p[c], __fmul_rn(k.half, k2[c]));
-    if (!sampler.sample(f, x, w)) return kStepOutOfBounds;
-    k3[0] = w[2]; k3[1] = w[1]; k3[2] = w[0];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) x[c] = __fadd_rn(p[c], __fmul_rn(k.dt, k3[c]));
-    if (!sampler.sample(f, x, w)) return kStepOutOfBounds;
-    k4[0] = w[2]; k4[1] = w[1]; k4[2] = w[0];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float t = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(p[c], __fmul_rn(k.c0, d[c])),
-                                                    __fmul_rn(k.c1, k2[c])),
-                                          __fmul_rn(k.c1, k3[c])),
-                                __fmul_rn(k.c0, k4[c]));
-      p[c] = t;
-    }
+    float2 k2_01, k3_01, k4_01;
+    float k2_2, k3_2, k4_2;
+    Position x;
+    x.p0 = __fadd_rn(p.p0, __fmul_rn(k.half, v2));
+    x.p21 = add2(p.p21, mul2(splat(k.half), v01));
+    if (!sampler.sample(f, x, k2_01, k2_2)) return kStepOutOfBounds;
+    x.p0 = __fadd_rn(p.p0, __fmul_rn(k.half, k2_2));
+    x.p21 = add2(p.p21, mul2(splat(k.half), k2_01));
+    if (!sampler.sample(f, x, k3_01, k3_2)) return kStepOutOfBounds;
+    x.p0 = __fadd_rn(p.p0, __fmul_rn(k.dt, k3_2));
+    x.p21 = add2(p.p21, mul2(splat(k.dt), k3_01));
+    if (!sampler.sample(f, x, k4_01, k4_2)) return kStepOutOfBounds;
+    p.p0 = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(p.p0, __fmul_rn(k.c0, v2)),
+                                         __fmul_rn(k.c1, k2_2)),
+                               __fmul_rn(k.c1, k3_2)),
+                     __fmul_rn(k.c0, k4_2));
+    const float2 C0 = splat(k.c0), C1 = splat(k.c1);
+    p.p21 = add2(add2(add2(add2(p.p21, mul2(C0, v01)), mul2(C1, k2_01)), mul2(C1, k3_01)),
+                 mul2(C0, k4_01));
   }
   return kStepTaken;
 }
