@@ -98,6 +98,8 @@ SIGNATURES = {
     "dpa_advect_device_no_alloc": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _P, _P,
                                              _P, _P]),
     "dpa_seed_lattice_device": (C.c_int, [_P, _F32P, _F32P, _F32P, _F32P, _U64P, _U64P, _P, _P]),
+    "dpa_seed_random_device": (C.c_int, [_P, _F32P, _F32P, C.c_uint64, C.c_uint64, _F32P, _U64P,
+                                         _P, _P]),
     "dpa_ftle_estimate": (C.c_int, [_P, _P, _F32P, C.c_uint64, C.c_float, C.c_uint64, _P, _P,
                                     C.c_int32, _P, _U64P]),
     "dpa_ftle_estimate_device": (C.c_int, [_P, _P, _F32P, C.c_uint64, C.c_float, C.c_uint64, _P,

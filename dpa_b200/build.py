@@ -5,6 +5,7 @@ pipeline.
 
 Outputs (git-ignored, shipped with the tree):
     dpa_b200/libdpa_b200.so     C ABI of include/dpa_b200.h (CUDA, sm_100a)
+    dpa_b200/libdpa_host.so     host pipeline, HDF5/XDMF, JSON (dpa_b200/host/dpa_host.h)
     dpa_b200/bin/dpa_pipeline   drop-in for the reference's `dpa config.json`
 """
 from __future__ import annotations
@@ -68,25 +69,40 @@ def build_library(force: bool = False, verbose_ptxas: bool = False) -> Path:
     return LIBRARY
 
 
-def build_pipeline(force: bool = False) -> Path | None:
-    sources = sorted(HOST.glob("*.cpp"))
-    if not sources:
-        return None
-    deps = sources + sorted(HOST.glob("*.hpp")) + [INCLUDE / "dpa_b200.h", LIBRARY]
-    if not force and not _stale(PIPELINE, deps):
-        return PIPELINE
-    PIPELINE.parent.mkdir(exist_ok=True)
-    cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", str(INCLUDE), "-I", str(HOST)]
-    cmd += [str(s) for s in sources]
-    cmd += ["-o", str(PIPELINE), "-L", str(PACKAGE), "-ldpa_b200",
-            "-Wl,-rpath,$ORIGIN/..", "-lpthread"]
-    _run(cmd)
-    return PIPELINE
+HOST_LIBRARY = PACKAGE / "libdpa_host.so"
+HOST_SOURCES = ["hdf5.cpp", "json.cpp", "pipeline.cpp", "host_api.cpp"]
+
+
+def host_compiler() -> str:
+    # The system g++ (the CXX of this image's environment may point at a
+    # toolchain without its support files).
+    return "/usr/bin/g++" if Path("/usr/bin/g++").exists() else (shutil.which("g++") or "g++")
+
+
+def build_host(force: bool = False) -> Path:
+    """libdpa_host.so (HDF5 / JSON / seeding / pipeline, C++17) and the
+    dpa_pipeline executable, both linked against libdpa_b200.so."""
+    sources = [HOST / s for s in HOST_SOURCES]
+    deps = sources + sorted(HOST.glob("*.hpp")) + sorted(HOST.glob("*.h")) + [
+        INCLUDE / "dpa_b200.h", LIBRARY]
+    if force or _stale(HOST_LIBRARY, deps):
+        tmp = HOST_LIBRARY.with_suffix(".so.tmp")
+        _run([host_compiler(), "-std=c++17", "-O2", "-Wall", "-fPIC", "-shared",
+              "-I", str(INCLUDE), "-I", str(HOST)] + [str(s) for s in sources] +
+             ["-o", str(tmp), "-L", str(PACKAGE), "-ldpa_b200", "-Wl,-rpath,$ORIGIN"])
+        os.replace(tmp, HOST_LIBRARY)
+    main = HOST / "main.cpp"
+    if force or _stale(PIPELINE, [main, HOST_LIBRARY, HOST / "pipeline.hpp"]):
+        PIPELINE.parent.mkdir(exist_ok=True)
+        _run([host_compiler(), "-std=c++17", "-O2", "-Wall", "-I", str(INCLUDE), "-I", str(HOST),
+              str(main), "-o", str(PIPELINE), "-L", str(PACKAGE), "-ldpa_host", "-ldpa_b200",
+              "-Wl,-rpath,$ORIGIN/.."])
+    return HOST_LIBRARY
 
 
 def build(force: bool = False) -> None:
     build_library(force=force)
-    build_pipeline(force=force)
+    build_host(force=force)
 
 
 if __name__ == "__main__":

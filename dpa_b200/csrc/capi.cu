@@ -633,6 +633,41 @@ int dpa_seed_lattice_device(dpa_context* ctx, const float offset_in[3], const fl
   });
 }
 
+int dpa_seed_random_device(dpa_context* ctx, const float offset_in[3], const float size_in[3],
+                           uint64_t count, uint64_t seed, const float* aabb, uint64_t* count_out,
+                           float* device_positions, void* stream) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  if (!offset_in || !size_in) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "NULL argument");
+  float offset[3] = {offset_in[0], offset_in[1], offset_in[2]};
+  float size[3] = {size_in[0], size_in[1], size_in[2]};
+  if (aabb) {
+    float lo[3], hi[3];
+    for (int i = 0; i < 3; ++i) {
+      lo[i] = std::max(aabb[i], offset[i]);
+      hi[i] = std::min(aabb[3 + i], offset[i] + size[i]);
+      if (lo[i] > hi[i]) count = 0;
+    }
+    if (count)
+      for (int i = 0; i < 3; ++i) {
+        offset[i] = lo[i];
+        size[i] = hi[i] - lo[i];
+      }
+  }
+  if (count_out) *count_out = count;
+  if (!device_positions || count == 0) return DPA_OK;
+  return guarded(ctx, [&]() -> int {
+    DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    uint64_t key = seed;
+    key += 0x9e3779b97f4a7c15ull;
+    key = (key ^ (key >> 30)) * 0xbf58476d1ce4e5b9ull;
+    key = (key ^ (key >> 27)) * 0x94d049bb133111ebull;
+    key ^= key >> 31;
+    DPA_TRY_CUDA(ctx, dpa::launch_random_seeds(offset, size, count, key, device_positions,
+                                               pick_stream(ctx, stream)));
+    return DPA_OK;
+  });
+}
+
 static int ftle_common(dpa_context* ctx, const dpa_field* field, const float seed_stride[3],
                        uint64_t iterations, float step_size, uint64_t count,
                        const float* original, const float* final_positions, int32_t mapping,

@@ -131,7 +131,37 @@ __global__ void lattice_kernel(float o0, float o1, float o2, float s0, float s1,
   out[3 * t + 2] = __fadd_rn(o2, __fmul_rn(s2, float(i2)));
 }
 
+// Counter-based seed stream: splitmix64 (Steele, Lea and Flood, "Fast
+// splittable pseudorandom number generators", 2014) of key ^ (3 i + axis).
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+  x += 0x9e3779b97f4a7c15ull;
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+  return x ^ (x >> 31);
+}
+
+__global__ void random_seeds_kernel(float o0, float o1, float o2, float s0, float s1, float s2,
+                                    uint64_t count, uint64_t key, float* out) {
+  const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= count) return;
+  const float o[3] = {o0, o1, o2}, s[3] = {s0, s1, s2};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const uint64_t r = splitmix64(key ^ (3 * t + uint64_t(a)));
+    const float u = float(uint32_t(r >> 40)) * 0x1p-24f;  // [0, 1), 24 random bits
+    out[3 * t + a] = __fadd_rn(o[a], __fmul_rn(s[a], u));
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_random_seeds(const float offset[3], const float size[3], uint64_t count,
+                                uint64_t key, float* out, cudaStream_t stream) {
+  if (count == 0) return cudaSuccess;
+  random_seeds_kernel<<<blocks_for(count, 256), 256, 0, stream>>>(
+      offset[0], offset[1], offset[2], size[0], size[1], size[2], count, key, out);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_ftle(const FtleArgs& a, cudaStream_t stream) {
   const uint64_t cells = a.shape[0] * a.shape[1] * a.shape[2];

@@ -82,6 +82,11 @@ struct FtleArgs {
 
 cudaError_t launch_ftle(const FtleArgs& a, cudaStream_t stream);
 
+// Uniform seeds offset + size * u, u from splitmix64(key ^ (3 i + axis)) >> 40
+// scaled by 2^-24; key = splitmix64(seed).
+cudaError_t launch_random_seeds(const float offset[3], const float size[3], uint64_t count,
+                                uint64_t key, float* out, cudaStream_t stream);
+
 cudaError_t launch_lattice_seeds(const float offset[3], const float stride[3],
                                  const uint64_t shape[3], float* out, cudaStream_t stream);
 

@@ -227,6 +227,18 @@ int dpa_seed_lattice_device(dpa_context* ctx, const float offset[3], const float
                             const float stride[3], const float* aabb, uint64_t* count,
                             uint64_t shape_out[3], float* device_positions, void* stream);
 
+/* Uniform random seeds on the device, for uniform_seed_generator::generate_random
+ * (uniform_seed_generator.cpp:46-81). The reference draws from a thread_local
+ * std::mt19937 seeded by std::random_device and can never repeat a seed set;
+ * here seed i, axis a is offset[a] + size[a] * u with
+ * u = (splitmix64(splitmix64(seed) ^ (3 i + a)) >> 40) * 2^-24 in [0, 1), so a
+ * (seed, count) pair always gives the same seeds, on any device or host.
+ * aabb clips the box as for the lattice; *count_out receives the count
+ * (0 when the clipped box is empty). */
+int dpa_seed_random_device(dpa_context* ctx, const float offset[3], const float size[3],
+                           uint64_t count, uint64_t seed, const float* aabb, uint64_t* count_out,
+                           float* device_positions, void* stream);
+
 /* ---- FTLE --------------------------------------------------------------------- */
 
 /* Replaces ftle_estimator::estimate (ftle_estimator.cpp:7-65): flow map of
