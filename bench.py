@@ -198,6 +198,42 @@ def fp64_error(a, ctx, field, grid, parts, sample=512, horizons=(50, 250, None))
     return out
 
 
+def precision_forms(a, ctx, grid, parts, p0, r0, pos, rem, term, stream, f32_kernel_ms,
+                    steps=5):
+    """The same workload with the field stored in FP16 and BF16 (FP32
+    interpolation and accumulation): kernel time, speed-up over this run's
+    FP32 kernel, and position error against the FP64 oracle."""
+    import ctypes as C
+    from dpa_b200 import _native as N
+    lib = ctx._lib
+    out = {}
+    for storage in ("f16", "bf16"):
+        if storage == a.storage:
+            continue
+        field = ctx.field(grid, storage)
+        opts = N.AdvectOptions(N.INTEGRATORS[a.integrator], float(np.float32(a.step_size)),
+                               0, 0, 0, 1)
+        times = []
+        for i in range(steps + 2):
+            pos.copy_(p0)
+            rem.copy_(r0)
+            ctx.check(lib.dpa_advect_device(ctx.handle, field.handle, C.byref(opts), a.seeds,
+                                            C.c_void_p(pos.data_ptr()), C.c_void_p(rem.data_ptr()),
+                                            C.c_void_p(term.data_ptr()),
+                                            C.c_void_p(stream.cuda_stream)))
+            o, k = C.c_float(), C.c_float()
+            ctx.check(lib.dpa_context_last_timing(ctx.handle, C.byref(o), C.byref(k)))
+            if i >= 2:
+                times.append(k.value)
+        steps_taken = float((a.iterations - rem.cpu().numpy().astype(np.int64)).sum())
+        kernel = statistics.mean(times)
+        out[storage] = {"kernel_ms": kernel, "particle_steps_per_s": steps_taken / (kernel / 1e3),
+                        "speedup_vs_f32_kernel": f32_kernel_ms / kernel,
+                        "fp64_error": fp64_error(a, ctx, field, grid, parts, horizons=(50, 250))}
+        field.close()
+    return out
+
+
 def run_reference(a):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -386,6 +422,8 @@ def run_gpu(a):
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(a, grid, parts, a.cpu_seconds)
         out["fp64_error"] = fp64_error(a, ctx, field, grid, parts)
+        out["precision_forms"] = precision_forms(a, ctx, grid, parts, pristine_pos, pristine_rem,
+                                                 pos, rem, term, stream, statistics.mean(kernel_ms))
     if rank == 0:
         print(json.dumps(out), flush=True)
     field.close()

@@ -36,7 +36,7 @@ INTEGRATORS = {
     "runge_kutta_4_true": 100,
 }
 
-TERMINATION = {0: "complete", 1: "out_of_bounds", 2: "zero_velocity"}
+TERMINATION = {0: "complete", 1: "out_of_bounds", 2: "zero_velocity", 3: "in_flight"}
 
 FTLE_MAPPING = {"reference": 0, "lattice": 1}
 
@@ -51,6 +51,7 @@ class AdvectOptions(C.Structure):
         ("index64", C.c_int32),
         ("colors", C.c_int32),
         ("morton_order", C.c_int32),
+        ("max_steps", C.c_uint64),
     ]
 
 
@@ -64,6 +65,77 @@ class CurveChunk(C.Structure):
         ("index_count", C.c_uint64),
         ("indices", C.c_void_p),
         ("last", C.c_int32),
+    ]
+
+
+class Tuning(C.Structure):
+    _fields_ = [
+        ("claim", C.c_uint32),
+        ("blocks_per_sm", C.c_uint32),
+        ("order", C.c_uint32),
+        ("measured_ms", C.c_float),
+    ]
+
+
+class ServerOptions(C.Structure):
+    _fields_ = [
+        ("particle_capacity", C.c_uint64),
+        ("vertex_capacity", C.c_uint64),
+        ("steps_per_tick", C.c_uint32),
+        ("max_requests", C.c_uint32),
+    ]
+
+
+class Request(C.Structure):
+    _fields_ = [
+        ("field", C.c_int32),
+        ("integrator", C.c_int32),
+        ("step_size", C.c_float),
+        ("record", C.c_int32),
+        ("index64", C.c_int32),
+        ("ftle", C.c_int32),
+        ("seed_stride", C.c_float * 3),
+        ("count", C.c_uint64),
+        ("positions", C.POINTER(C.c_float)),
+        ("iterations", C.c_uint64),
+        ("user", C.c_void_p),
+    ]
+
+
+class Response(C.Structure):
+    _fields_ = [
+        ("id", C.c_uint64),
+        ("user", C.c_void_p),
+        ("status", C.c_int32),
+        ("count", C.c_uint64),
+        ("positions", C.POINTER(C.c_float)),
+        ("remaining", C.POINTER(C.c_uint64)),
+        ("termination", C.POINTER(C.c_uint8)),
+        ("vertex_count", C.c_uint64),
+        ("vertices", C.POINTER(C.c_float)),
+        ("colors", C.POINTER(C.c_float)),
+        ("index_count", C.c_uint64),
+        ("indices", C.c_void_p),
+        ("ftle_shape", C.c_uint64 * 3),
+        ("ftle", C.POINTER(C.c_float)),
+        ("particle_steps", C.c_uint64),
+        ("queued_seconds", C.c_double),
+        ("admitted_seconds", C.c_double),
+        ("finished_seconds", C.c_double),
+    ]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_uint64),
+        ("admitted", C.c_uint64),
+        ("completed", C.c_uint64),
+        ("ticks", C.c_uint64),
+        ("launches", C.c_uint64),
+        ("particle_steps", C.c_uint64),
+        ("busy_seconds", C.c_double),
+        ("queued", C.c_uint32),
+        ("active", C.c_uint32),
     ]
 
 
@@ -95,6 +167,23 @@ SIGNATURES = {
     "dpa_advect_round": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _P, _P, _P,
                                    CURVE_SINK, _P]),
     "dpa_advect_device": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _P, _P, _P, _P]),
+    "dpa_advect_batch_device": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _U64P,
+                                          _P, _P, _P, _U64P, _P]),
+    "dpa_graph_create_advect": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _P, _P,
+                                          _P, C.POINTER(C.c_void_p)]),
+    "dpa_graph_launch": (C.c_int, [_P, _P, _P]),
+    "dpa_graph_destroy": (C.c_int, [_P, _P]),
+    "dpa_context_set_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "dpa_context_get_tuning": (C.c_int, [_P, C.POINTER(Tuning)]),
+    "dpa_autotune_advect": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _P, _P,
+                                      C.c_uint64, C.POINTER(Tuning)]),
+    "dpa_server_create": (C.c_int, [_P, C.POINTER(ServerOptions), C.POINTER(C.c_void_p)]),
+    "dpa_server_add_field": (C.c_int, [_P, _P, C.POINTER(C.c_int32)]),
+    "dpa_server_submit": (C.c_int, [_P, C.POINTER(Request), _U64P]),
+    "dpa_server_poll": (C.c_int, [_P, C.c_int32, C.POINTER(Response), C.POINTER(C.c_int32)]),
+    "dpa_server_release": (C.c_int, [_P, C.c_uint64]),
+    "dpa_server_get_stats": (C.c_int, [_P, C.POINTER(ServerStats)]),
+    "dpa_server_destroy": (C.c_int, [_P]),
     "dpa_advect_device_no_alloc": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _P, _P,
                                              _P, _P]),
     "dpa_seed_lattice_device": (C.c_int, [_P, _F32P, _F32P, _F32P, _F32P, _U64P, _U64P, _P, _P]),

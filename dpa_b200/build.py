@@ -25,7 +25,7 @@ LIBRARY = PACKAGE / "libdpa_b200.so"
 PIPELINE = PACKAGE / "bin" / "dpa_pipeline"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SOURCES = ["capi.cu", "advect.cu", "emit.cu", "ftle.cu", "noalloc.cu"]
+CUDA_SOURCES = ["capi.cu", "advect.cu", "emit.cu", "ftle.cu", "noalloc.cu", "serve.cu"]
 
 
 def nvcc() -> str:

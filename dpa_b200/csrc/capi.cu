@@ -15,6 +15,13 @@
 #include "handles.cuh"
 #include "kernels.cuh"
 
+struct dpa_graph {
+  dpa_context* owner = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t launches = 0;  // kernels per replay
+};
+
 namespace {
 
 int fail(dpa_context* ctx, int status, const std::string& message) {
@@ -81,6 +88,8 @@ int check_options(dpa_context* ctx, const dpa_advect_options* o) {
   }
   if (!std::isfinite(o->step_size))
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "step_size is not finite");
+  if (o->record && o->max_steps)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "max_steps applies to calls without recording");
   return DPA_OK;
 }
 
@@ -95,7 +104,7 @@ int build_order(dpa_context* ctx, const dpa_field* field, const float* positions
   DPA_TRY_CUDA(ctx, ctx->sort_temp.reserve((dpa::kOrderBuckets + 1) * 4));
   DPA_TRY_CUDA(ctx, dpa::launch_order(field->view, positions, count, ctx->keys.as<uint16_t>(),
                                       ctx->sort_temp.as<uint32_t>(), ctx->values.as<uint32_t>(),
-                                      stream));
+                                      stream, ctx->tuning.order));
   ctx->launches += dpa::kOrderLaunches;
   *order = ctx->values.as<uint32_t>();
   return DPA_OK;
@@ -108,13 +117,17 @@ int advect_device_impl(dpa_context* ctx, const dpa_field* field, const dpa_advec
   if (count == 0) return DPA_OK;
   if (ctx->profiling) DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->events[0], s));
   const uint32_t* order = nullptr;
-  if (o->morton_order) {
+  if (o->morton_order && ctx->tuning.order) {
     const int st = build_order(ctx, field, positions, count, s, &order);
     if (st != DPA_OK) return st;
   }
   if (ctx->profiling) DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->events[1], s));
   DPA_TRY_CUDA(ctx, ctx->work_counter.reserve(sizeof(unsigned long long)));
   dpa::AdvectArgs a{};
+  dpa::set_launch_defaults(a);
+  if (o->max_steps) a.max_steps = o->max_steps;
+  a.claim = ctx->tuning.claim;
+  a.blocks_per_sm = ctx->tuning.blocks_per_sm;
   a.work_counter = ctx->work_counter.as<unsigned long long>();
   a.count = count;
   a.order = order;
@@ -173,12 +186,15 @@ int record_piece(dpa_context* ctx, const dpa_field* field, const dpa_advect_opti
   uint64_t* remaining = ctx->remaining.as<uint64_t>() + begin;
   uint8_t* termination = ctx->termination.as<uint8_t>() + begin;
   const uint32_t* order = nullptr;
-  if (o->morton_order) {
+  if (o->morton_order && ctx->tuning.order) {
     const int st = build_order(ctx, field, positions, n, s, &order);
     if (st != DPA_OK) return st;
   }
   DPA_TRY_CUDA(ctx, ctx->work_counter.reserve(sizeof(unsigned long long)));
   dpa::AdvectArgs a{};
+  dpa::set_launch_defaults(a);
+  a.claim = ctx->tuning.claim;
+  a.blocks_per_sm = ctx->tuning.blocks_per_sm;
   a.work_counter = ctx->work_counter.as<unsigned long long>();
   a.count = n;
   a.order = order;
@@ -763,6 +779,228 @@ int dpa_ftle_estimate_device(dpa_context* ctx, const dpa_field* field, const flo
     DPA_TRY_CUDA(ctx, dpa::launch_ftle(a, s));
     return DPA_OK;
   });
+}
+
+int dpa_context_set_tuning(dpa_context* ctx, const dpa_tuning* tuning) {
+  if (!ctx || !tuning) return DPA_ERROR_INVALID_ARGUMENT;
+  if (tuning->claim < 1 || tuning->claim > 4096)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "claim must be in [1, 4096]");
+  if (tuning->order > 16)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "order resolution must be in [0, 16]");
+  ctx->tuning.claim = tuning->claim;
+  ctx->tuning.blocks_per_sm = tuning->blocks_per_sm;
+  ctx->tuning.order = tuning->order;
+  return DPA_OK;
+}
+
+int dpa_context_get_tuning(const dpa_context* ctx, dpa_tuning* tuning) {
+  if (!ctx || !tuning) return DPA_ERROR_INVALID_ARGUMENT;
+  tuning->claim = ctx->tuning.claim;
+  tuning->blocks_per_sm = ctx->tuning.blocks_per_sm;
+  tuning->order = ctx->tuning.order;
+  tuning->measured_ms = 0.0f;
+  return DPA_OK;
+}
+
+int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_advect_options* options,
+                        uint64_t count, const float* device_positions,
+                        const uint64_t* device_remaining, uint64_t sample_steps,
+                        dpa_tuning* best) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  int st = check_options(ctx, options);
+  if (st != DPA_OK) return st;
+  if (options->record)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "autotune measures calls without recording");
+  if (!field || field->owner != ctx) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "bad field");
+  if (count == 0 || !device_positions || !device_remaining)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "autotune needs particles");
+  return guarded(ctx, [&]() -> int {
+    DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    // A sample of the particles, run for at most sample_steps steps each.
+    const uint64_t n = std::min<uint64_t>(count, 1ull << 18);
+    DeviceBuffer pos, rem, pos0, rem0, term;
+    DPA_TRY_CUDA(ctx, pos.reserve(n * 12));
+    DPA_TRY_CUDA(ctx, rem.reserve(n * 8));
+    DPA_TRY_CUDA(ctx, pos0.reserve(n * 12));
+    DPA_TRY_CUDA(ctx, rem0.reserve(n * 8));
+    DPA_TRY_CUDA(ctx, term.reserve(n));
+    DPA_TRY_CUDA(ctx, cudaMemcpyAsync(pos0.ptr, device_positions, n * 12, cudaMemcpyDeviceToDevice, s));
+    DPA_TRY_CUDA(ctx, cudaMemcpyAsync(rem0.ptr, device_remaining, n * 8, cudaMemcpyDeviceToDevice, s));
+    dpa_advect_options o = *options;
+    o.max_steps = sample_steps ? sample_steps : 200;
+    cudaEvent_t e0, e1;
+    DPA_TRY_CUDA(ctx, cudaEventCreate(&e0));
+    DPA_TRY_CUDA(ctx, cudaEventCreate(&e1));
+    const dpa_tuning_state saved = ctx->tuning;
+    const bool profiling = ctx->profiling;
+    ctx->profiling = false;
+    dpa_tuning_state winner = saved;
+    float winner_ms = 0.0f;
+    bool first = true;
+    int rc = DPA_OK;
+    const uint32_t claims[] = {16, 32, 64, 128};
+    const uint32_t grids[] = {0, 3, 2};
+    const uint32_t orders[] = {16, 8, 0};
+    for (uint32_t order : orders)
+      for (uint32_t grid : grids)
+        for (uint32_t claim : claims) {
+          ctx->tuning = {claim, grid, order};
+          float best_ms = 0.0f;
+          for (int rep = 0; rep < 3 && rc == DPA_OK; ++rep) {
+            cudaMemcpyAsync(pos.ptr, pos0.ptr, n * 12, cudaMemcpyDeviceToDevice, s);
+            cudaMemcpyAsync(rem.ptr, rem0.ptr, n * 8, cudaMemcpyDeviceToDevice, s);
+            cudaEventRecord(e0, s);
+            rc = advect_device_impl(ctx, field, &o, n, pos.as<float>(), rem.as<uint64_t>(),
+                                    term.as<uint8_t>(), s);
+            cudaEventRecord(e1, s);
+            cudaEventSynchronize(e1);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (rep > 0 && (best_ms == 0.0f || ms < best_ms)) best_ms = ms;
+          }
+          if (rc != DPA_OK) break;
+          if (first || best_ms < winner_ms) {
+            winner = ctx->tuning;
+            winner_ms = best_ms;
+            first = false;
+          }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->profiling = profiling;
+    ctx->tuning = rc == DPA_OK ? winner : saved;
+    if (rc != DPA_OK) return rc;
+    if (best) {
+      best->claim = winner.claim;
+      best->blocks_per_sm = winner.blocks_per_sm;
+      best->order = winner.order;
+      best->measured_ms = winner_ms;
+    }
+    return DPA_OK;
+  });
+}
+
+int dpa_advect_batch_device(dpa_context* ctx, const dpa_field* field,
+                            const dpa_advect_options* options, uint64_t set_count,
+                            const uint64_t* set_offsets, float* device_positions,
+                            uint64_t* device_remaining, uint8_t* device_termination,
+                            uint64_t* set_steps, void* stream) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  int st = check_options(ctx, options);
+  if (st != DPA_OK) return st;
+  if (options->record)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "batched launches do not record");
+  if (!field || field->owner != ctx) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "bad field");
+  if (set_count && !set_offsets) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "set_offsets is NULL");
+  for (uint64_t i = 0; i < set_count; ++i)
+    if (set_offsets[i + 1] < set_offsets[i])
+      return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "set_offsets must not decrease");
+  const uint64_t total = set_count ? set_offsets[set_count] - set_offsets[0] : 0;
+  if (set_count && set_offsets[0] != 0)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "set_offsets must start at 0");
+  if (total > 0xffffffffull)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "at most 2^32-1 particles per batch");
+  if (total && (!device_positions || !device_remaining))
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "positions or remaining is NULL");
+  return guarded(ctx, [&]() -> int {
+    DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = pick_stream(ctx, stream);
+    if (set_steps) {
+      DPA_TRY_CUDA(ctx, ctx->remaining_in.reserve(total * 8 + 8));
+      DPA_TRY_CUDA(ctx, ctx->raw_offsets.reserve((set_count + 1) * 8));
+      DPA_TRY_CUDA(ctx, ctx->wide.reserve(set_count * 8 + 8));
+      DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->remaining_in.ptr, device_remaining, total * 8,
+                                        cudaMemcpyDeviceToDevice, s));
+    }
+    // One persistent launch over every set: each particle carries its own
+    // remaining iteration count, so sets of any size and iteration count mix.
+    st = advect_device_impl(ctx, field, options, total, device_positions, device_remaining,
+                            device_termination, s);
+    if (st != DPA_OK) return st;
+    if (set_steps && set_count) {
+      DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->raw_offsets.ptr, set_offsets, (set_count + 1) * 8,
+                                        cudaMemcpyHostToDevice, s));
+      DPA_TRY_CUDA(ctx, dpa::launch_set_steps(ctx->remaining_in.as<uint64_t>(), device_remaining,
+                                              ctx->raw_offsets.as<uint64_t>(), set_count,
+                                              ctx->wide.as<unsigned long long>(), s));
+      DPA_TRY_CUDA(ctx, cudaMemcpyAsync(set_steps, ctx->wide.ptr, set_count * 8,
+                                        cudaMemcpyDeviceToHost, s));
+      DPA_TRY_CUDA(ctx, cudaStreamSynchronize(s));
+    }
+    return DPA_OK;
+  });
+}
+
+int dpa_graph_create_advect(dpa_context* ctx, const dpa_field* field,
+                            const dpa_advect_options* options, uint64_t count,
+                            float* device_positions, uint64_t* device_remaining,
+                            uint8_t* device_termination, dpa_graph** out) {
+  if (!ctx || !out) return DPA_ERROR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int st = check_options(ctx, options);
+  if (st != DPA_OK) return st;
+  if (options->record) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "graphs do not record");
+  if (!field || field->owner != ctx) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "bad field");
+  if (count == 0 || count > 0xffffffffull || !device_positions || !device_remaining)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "graphs need 1 to 2^32-1 particles");
+  return guarded(ctx, [&]() -> int {
+    DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    // Everything the launch sequence allocates or looks up, before capture.
+    DPA_TRY_CUDA(ctx, ctx->keys.reserve(count * 2));
+    DPA_TRY_CUDA(ctx, ctx->values.reserve(count * 4));
+    DPA_TRY_CUDA(ctx, ctx->sort_temp.reserve((dpa::kOrderBuckets + 1) * 4));
+    DPA_TRY_CUDA(ctx, ctx->work_counter.reserve(sizeof(unsigned long long)));
+    DPA_TRY_CUDA(ctx, dpa::prepare_advect(field->view, options->integrator, false));
+    DPA_TRY_CUDA(ctx, cudaStreamSynchronize(s));
+    const bool profiling = ctx->profiling;
+    ctx->profiling = false;
+    const uint64_t launches0 = ctx->launches;
+    cudaGraph_t graph = nullptr;
+    DPA_TRY_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    st = advect_device_impl(ctx, field, options, count, device_positions, device_remaining,
+                            device_termination, s);
+    const cudaError_t end = cudaStreamEndCapture(s, &graph);
+    ctx->profiling = profiling;
+    if (st != DPA_OK) {
+      if (graph) cudaGraphDestroy(graph);
+      return st;
+    }
+    if (end != cudaSuccess) return fail_cuda(ctx, end, "cudaStreamEndCapture");
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t inst = cudaGraphInstantiate(&exec, graph, 0);
+    if (inst != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      return fail_cuda(ctx, inst, "cudaGraphInstantiate");
+    }
+    dpa_graph* g = new dpa_graph();
+    g->owner = ctx;
+    g->graph = graph;
+    g->exec = exec;
+    g->launches = ctx->launches - launches0;
+    ctx->launches = launches0;  // capture launched nothing
+    *out = g;
+    return DPA_OK;
+  });
+}
+
+int dpa_graph_launch(dpa_context* ctx, dpa_graph* graph, void* stream) {
+  if (!ctx || !graph || graph->owner != ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+  DPA_TRY_CUDA(ctx, cudaGraphLaunch(graph->exec, pick_stream(ctx, stream)));
+  ctx->launches += graph->launches;
+  return DPA_OK;
+}
+
+int dpa_graph_destroy(dpa_context* ctx, dpa_graph* graph) {
+  if (!ctx || !graph || graph->owner != ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  if (graph->exec) cudaGraphExecDestroy(graph->exec);
+  if (graph->graph) cudaGraphDestroy(graph->graph);
+  delete graph;
+  return DPA_OK;
 }
 
 }  // extern "C"

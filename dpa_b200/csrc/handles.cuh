@@ -8,9 +8,15 @@
 
 namespace dpa {
 
+// Grow-only device buffer; freed by release() or when it goes out of scope
+// (with its device current).
 struct DeviceBuffer {
   void* ptr = nullptr;
   size_t bytes = 0;
+  DeviceBuffer() = default;
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  ~DeviceBuffer() { release(); }
   cudaError_t reserve(size_t n) {
     if (n <= bytes && ptr) return cudaSuccess;
     release();
@@ -35,6 +41,10 @@ struct DeviceBuffer {
 struct PinnedBuffer {
   void* ptr = nullptr;
   size_t bytes = 0;
+  PinnedBuffer() = default;
+  PinnedBuffer(const PinnedBuffer&) = delete;
+  PinnedBuffer& operator=(const PinnedBuffer&) = delete;
+  ~PinnedBuffer() { release(); }
   cudaError_t reserve(size_t n) {
     if (n <= bytes && ptr) return cudaSuccess;
     release();
@@ -61,6 +71,14 @@ struct PinnedBuffer {
 using dpa::DeviceBuffer;
 using dpa::PinnedBuffer;
 
+// Launch parameters an autotuner may change per context.
+struct dpa_tuning_state {
+  uint32_t claim = 32;        // order entries a warp claims at once
+  uint32_t blocks_per_sm = 0; // persistent grid: 0 = as many as fit
+  uint32_t order = 16;        // processing order: Morton buckets of an order^3
+                              // coarsening of the grid (1..16); 0: input order
+};
+
 struct dpa_context {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -73,6 +91,7 @@ struct dpa_context {
   bool profiling = false;
   cudaEvent_t events[3] = {nullptr, nullptr, nullptr};  // order, advect begin, advect end
   bool timed_order = false;
+  dpa_tuning_state tuning;
   DeviceBuffer raw, raw_offsets, raw_counts, kept_vertices, kept_segments;
   DeviceBuffer wide, vertex_offsets, segment_offsets, scan_temp, totals;
   DeviceBuffer out_vertices, out_colors, out_indices;

@@ -18,16 +18,46 @@ struct AdvectArgs {
   uint64_t* remaining;    // [count], updated in place
   uint8_t* termination;   // [count] or null
   StepCoefficients coefficients;
+  uint64_t max_steps;                // step budget of this launch (~0: none)
+  uint32_t claim;                    // order entries a warp claims at once
+  uint32_t blocks_per_sm;            // persistent grid per SM (0: occupancy maximum)
   unsigned long long* work_counter;  // zeroed by the launcher; claims of the order
   // Recording only.
   float* raw_vertices;          // unpruned curve of particle k at raw_offsets[k]
   const uint64_t* raw_offsets;  // exclusive scan of remaining + 2
   uint32_t* kept_vertices;      // per particle: vertices surviving the prune
   uint32_t* kept_segments;      // per particle: index pairs it contributes
+  // Resumed recording (null for a curve recorded in one launch).
+  const uint64_t* remaining_initial;  // remaining iterations when the curve began
+  uint8_t* curve_open;                // last kept vertex is not terminal-valued
+  // Serving: skip order entries whose termination is not in flight, and count
+  // each particle's finish down in its request's counter (null when unused).
+  bool resume_only;
+  const uint32_t* request_of;         // per particle
+  unsigned int* in_flight;            // per request
 };
+
+// Launch defaults: no step budget, 32-entry claims.
+inline void set_launch_defaults(AdvectArgs& a) {
+  a.max_steps = ~0ull;
+  a.claim = 32;
+  a.blocks_per_sm = 0;
+  a.resume_only = false;
+  a.request_of = nullptr;
+  a.in_flight = nullptr;
+}
+
+// list[t] = starts[r] + (t - firsts[r]) for the range r holding t, where
+// firsts is the exclusive scan of the range lengths (ranges of arena slots).
+cudaError_t launch_expand_ranges(const uint64_t* starts, const uint64_t* firsts, uint32_t ranges,
+                                 uint64_t total, uint32_t* list, cudaStream_t stream);
 
 cudaError_t launch_advect(const FieldView& f, const AdvectArgs& a, int integrator, bool record,
                           cudaStream_t stream);
+
+// Resolves, outside any stream capture, what launch_advect looks up on its
+// first use of a kernel instantiation (its occupancy).
+cudaError_t prepare_advect(const FieldView& f, int integrator, bool record);
 
 // Processing order: a counting sort of the particles by the Morton code of
 // their start cell on a 16^3 coarsening of the grid (four kernels). Within a
@@ -36,7 +66,14 @@ constexpr int kOrderBuckets = 4096;
 constexpr int kOrderLaunches = 4;
 
 cudaError_t launch_order(const FieldView& f, const float* positions, uint64_t count,
-                         uint16_t* buckets, uint32_t* counts, uint32_t* order, cudaStream_t stream);
+                         uint16_t* buckets, uint32_t* counts, uint32_t* order, cudaStream_t stream,
+                         uint32_t resolution = 16);
+
+// Particle-steps each seed set took: sum over [offsets[s], offsets[s+1]) of
+// remaining_in - remaining_out.
+cudaError_t launch_set_steps(const uint64_t* remaining_in, const uint64_t* remaining_out,
+                             const uint64_t* offsets, uint64_t sets, unsigned long long* steps,
+                             cudaStream_t stream);
 
 struct EmitArgs {
   uint64_t count;                 // particles in this piece, in round order

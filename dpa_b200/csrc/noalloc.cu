@@ -113,6 +113,8 @@ extern "C" int dpa_advect_device_no_alloc(dpa_context* ctx, const dpa_field* fie
       order = order_out;
     }
     dpa::AdvectArgs a{};
+    dpa::set_launch_defaults(a);
+    if (options->max_steps) a.max_steps = options->max_steps;
     // launch_advect zeroes the work counter before the kernel starts.
     a.work_counter = reinterpret_cast<unsigned long long*>(scratch + kCounterOffset);
     a.count = count;

@@ -1,0 +1,637 @@
+// serve.cu -- the request server: resident fields, admission by device
+// memory, continuous batching of advection / FTLE requests.
+//
+// No counterpart in the reference (a batch MPI program). A worker thread owns
+// two device arenas: particle slots (position, remaining iterations and the
+// per-particle state of resumable launches) and raw curve staging (the
+// unpruned vertices of recording requests, remaining + 2 per particle). A
+// request is admitted, first in first out, when the arenas have room for it:
+// its seeds take `count` slots, and a recording request also takes
+// count * (iterations + 2) staging vertices -- its output buffer. Admitted
+// requests advance together: each tick is one persistent advection launch per
+// (field, integrator, step, recording) group over every in-flight particle of
+// the group's requests, with a step budget, so requests that arrive while
+// others run join at the next tick and share the launches. A request whose
+// particles have all finished is emitted (curve, FTLE) and returned.
+#include <cub/device/device_scan.cuh>
+
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <tuple>
+#include <vector>
+
+#include "handles.cuh"
+#include "kernels.cuh"
+
+namespace {
+
+using clock_type = std::chrono::steady_clock;
+
+// First-fit allocator of [0, capacity) ranges, coalescing on free.
+class range_allocator {
+ public:
+  explicit range_allocator(uint64_t capacity = 0) { reset(capacity); }
+  void reset(uint64_t capacity) {
+    free_.clear();
+    if (capacity) free_[0] = capacity;
+    capacity_ = capacity;
+  }
+  bool allocate(uint64_t n, uint64_t* offset) {
+    if (n == 0) {
+      *offset = 0;
+      return true;
+    }
+    for (auto it = free_.begin(); it != free_.end(); ++it) {
+      if (it->second >= n) {
+        *offset = it->first;
+        const uint64_t rest = it->second - n;
+        const uint64_t at = it->first + n;
+        free_.erase(it);
+        if (rest) free_[at] = rest;
+        return true;
+      }
+    }
+    return false;
+  }
+  void release(uint64_t offset, uint64_t n) {
+    if (n == 0) return;
+    auto next = free_.lower_bound(offset);
+    if (next != free_.end() && offset + n == next->first) {
+      n += next->second;
+      next = free_.erase(next);
+    }
+    if (next != free_.begin()) {
+      auto prev = std::prev(next);
+      if (prev->first + prev->second == offset) {
+        prev->second += n;
+        return;
+      }
+    }
+    free_[offset] = n;
+  }
+
+ private:
+  std::map<uint64_t, uint64_t> free_;
+  uint64_t capacity_ = 0;
+};
+
+struct pending {
+  uint64_t id;
+  dpa_request request;
+  std::vector<float> positions;
+  double queued;
+};
+
+struct active_request {
+  pending p;
+  uint32_t slot;         // index of its in-flight counter
+  uint64_t first;        // first particle slot
+  uint64_t raw_first;    // first staging vertex (recording)
+  uint64_t raw_count;
+  double admitted;
+};
+
+struct response_storage {
+  dpa_response r{};
+  std::vector<float> positions, vertices, colors, ftle;
+  std::vector<uint64_t> remaining, indices64;
+  std::vector<uint32_t> indices32;
+  std::vector<uint8_t> termination;
+};
+
+}  // namespace
+
+struct dpa_server {
+  dpa_context* ctx = nullptr;
+  dpa_server_options options{};
+  std::vector<const dpa_field*> fields;
+  cudaStream_t stream = nullptr;
+
+  // Particle arena (per slot) and curve staging arena (per vertex).
+  DeviceBuffer positions, remaining, remaining_initial, termination, raw_offsets, kept_vertices,
+      kept_segments, curve_open, request_of, raw, in_flight;
+  // Per tick.
+  DeviceBuffer list, starts, firsts, work_counter;
+  PinnedBuffer host_ranges, host_in_flight;
+  // Emission scratch.
+  DeviceBuffer raw_counts, wide, vertex_offsets, segment_offsets, scan_temp, out_vertices,
+      out_colors, out_indices;
+  DeviceBuffer ftle_original, ftle_winners, ftle_flow, ftle_out;
+  range_allocator slots, vertices;
+  std::vector<uint32_t> free_counters;
+
+  std::mutex mutex;
+  std::condition_variable wake, done_signal;
+  std::deque<pending> queue;
+  std::vector<active_request> active;
+  std::map<uint64_t, std::unique_ptr<response_storage>> done, handed_out;
+  std::deque<uint64_t> done_order;
+  std::thread worker;
+  bool stopping = false;
+  std::string failure;
+  uint64_t next_id = 1;
+  dpa_server_stats stats{};
+  clock_type::time_point start = clock_type::now();
+
+  double now() const { return std::chrono::duration<double>(clock_type::now() - start).count(); }
+  void run();
+  bool tick();
+  void select(std::vector<active_request>& out);
+  void upload(const active_request& a);
+  void finish(active_request& a, response_storage& out);
+};
+
+namespace {
+
+#define SERVER_TRY(expr)                                                   \
+  do {                                                                     \
+    const cudaError_t e_ = (expr);                                         \
+    if (e_ != cudaSuccess)                                                 \
+      throw std::runtime_error(std::string(#expr) + ": " + cudaGetErrorName(e_)); \
+  } while (0)
+
+bool integrator_ok(int32_t i) {
+  return i == DPA_INTEGRATOR_EULER || i == DPA_INTEGRATOR_RUNGE_KUTTA_4 ||
+         i == DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE;
+}
+
+}  // namespace
+
+// Called with the mutex held: moves the queue's head requests that fit the
+// arenas into `out`, first in, first out (the head waits until they have
+// room for it).
+void dpa_server::select(std::vector<active_request>& out) {
+  while (!queue.empty() && !free_counters.empty()) {
+    pending& head = queue.front();
+    const dpa_request& q = head.request;
+    const uint64_t raw_need = q.record ? q.count * (q.iterations + 2) : 0;
+    uint64_t first = 0, raw_first = 0;
+    if (!slots.allocate(q.count, &first)) break;
+    if (!vertices.allocate(raw_need, &raw_first)) {
+      slots.release(first, q.count);
+      break;
+    }
+    active_request a;
+    a.p = std::move(head);
+    queue.pop_front();
+    a.slot = free_counters.back();
+    free_counters.pop_back();
+    a.first = first;
+    a.raw_first = raw_first;
+    a.raw_count = raw_need;
+    a.admitted = now();
+    out.push_back(std::move(a));
+  }
+}
+
+// Uploads an admitted request's seeds and resumable state (every particle in
+// flight); worker thread, without the mutex.
+void dpa_server::upload(const active_request& a) {
+  const dpa_request& q = a.p.request;
+  const uint64_t n = q.count, first = a.first;
+  const unsigned int count32 = unsigned(n);
+  SERVER_TRY(cudaMemcpyAsync(in_flight.as<unsigned int>() + a.slot, &count32, 4,
+                             cudaMemcpyHostToDevice, stream));
+  if (n) {
+    SERVER_TRY(cudaMemcpyAsync(positions.as<float>() + 3 * first, a.p.positions.data(), n * 12,
+                               cudaMemcpyHostToDevice, stream));
+    std::vector<uint64_t> rem(n, q.iterations), raw_off;
+    std::vector<uint32_t> owner(n, a.slot);
+    SERVER_TRY(cudaMemcpyAsync(remaining.as<uint64_t>() + first, rem.data(), n * 8,
+                               cudaMemcpyHostToDevice, stream));
+    SERVER_TRY(cudaMemcpyAsync(remaining_initial.as<uint64_t>() + first, rem.data(), n * 8,
+                               cudaMemcpyHostToDevice, stream));
+    SERVER_TRY(cudaMemsetAsync(termination.as<uint8_t>() + first, DPA_TERMINATION_IN_FLIGHT, n,
+                               stream));
+    SERVER_TRY(cudaMemcpyAsync(request_of.as<uint32_t>() + first, owner.data(), n * 4,
+                               cudaMemcpyHostToDevice, stream));
+    if (q.record) {
+      raw_off.resize(n);
+      for (uint64_t i = 0; i < n; ++i) raw_off[i] = a.raw_first + i * (q.iterations + 2);
+      SERVER_TRY(cudaMemcpyAsync(raw_offsets.as<uint64_t>() + first, raw_off.data(), n * 8,
+                                 cudaMemcpyHostToDevice, stream));
+    }
+    // The host vectors above die at the end of this scope: wait for them.
+    SERVER_TRY(cudaStreamSynchronize(stream));
+  } else {
+    SERVER_TRY(cudaStreamSynchronize(stream));
+  }
+}
+
+// One tick: a step-budgeted launch per group of requests that can share one.
+// Returns false when nothing was in flight.
+bool dpa_server::tick() {
+  using key_type = std::tuple<int32_t, int32_t, float, int32_t>;  // field, integrator, step, record
+  std::map<key_type, std::vector<const active_request*>> groups;
+  for (const active_request& a : active) {
+    const dpa_request& q = a.p.request;
+    if (q.count == 0) continue;
+    groups[{q.field, q.integrator, q.step_size, q.record ? 1 : 0}].push_back(&a);
+  }
+  if (groups.empty()) return false;
+  for (auto& [key, members] : groups) {
+    const auto [field_id, integrator, step_size, record] = key;
+    const dpa_field* field = fields[size_t(field_id)];
+    const uint32_t ranges = uint32_t(members.size());
+    SERVER_TRY(host_ranges.reserve(uint64_t(ranges) * 16));
+    SERVER_TRY(starts.reserve(uint64_t(ranges) * 8));
+    SERVER_TRY(firsts.reserve(uint64_t(ranges) * 8));
+    uint64_t* h = host_ranges.as<uint64_t>();
+    uint64_t total = 0;
+    for (uint32_t r = 0; r < ranges; ++r) {
+      h[r] = members[r]->first;
+      h[ranges + r] = total;
+      total += members[r]->p.request.count;
+    }
+    SERVER_TRY(list.reserve(total * 4));
+    SERVER_TRY(cudaMemcpyAsync(starts.ptr, h, uint64_t(ranges) * 8, cudaMemcpyHostToDevice, stream));
+    SERVER_TRY(cudaMemcpyAsync(firsts.ptr, h + ranges, uint64_t(ranges) * 8, cudaMemcpyHostToDevice,
+                               stream));
+    SERVER_TRY(dpa::launch_expand_ranges(starts.as<uint64_t>(), firsts.as<uint64_t>(), ranges,
+                                         total, list.as<uint32_t>(), stream));
+    dpa::AdvectArgs a{};
+    dpa::set_launch_defaults(a);
+    a.count = total;
+    a.order = list.as<uint32_t>();
+    a.positions = positions.as<float>();
+    a.remaining = remaining.as<uint64_t>();
+    a.termination = termination.as<uint8_t>();
+    a.coefficients = dpa::make_step_coefficients(step_size);
+    a.max_steps = options.steps_per_tick ? options.steps_per_tick : 64;
+    a.claim = ctx->tuning.claim;
+    a.work_counter = work_counter.as<unsigned long long>();
+    a.resume_only = true;
+    a.request_of = request_of.as<uint32_t>();
+    a.in_flight = in_flight.as<unsigned int>();
+    if (record) {
+      a.raw_vertices = raw.as<float>();
+      a.raw_offsets = raw_offsets.as<uint64_t>();
+      a.kept_vertices = kept_vertices.as<uint32_t>();
+      a.kept_segments = kept_segments.as<uint32_t>();
+      a.remaining_initial = remaining_initial.as<uint64_t>();
+      a.curve_open = curve_open.as<uint8_t>();
+    }
+    SERVER_TRY(dpa::launch_advect(field->view, a, integrator, record != 0, stream));
+    stats.launches += 1;
+    // (The host ranges are rewritten by the next group: wait for this copy.)
+    SERVER_TRY(cudaStreamSynchronize(stream));
+  }
+  stats.ticks += 1;
+  return true;
+}
+
+void dpa_server::finish(active_request& a, response_storage& out) {
+  const dpa_request& q = a.p.request;
+  const uint64_t n = q.count, first = a.first;
+  out.positions.resize(3 * n);
+  out.remaining.resize(n);
+  out.termination.resize(n);
+  if (n) {
+    SERVER_TRY(cudaMemcpyAsync(out.positions.data(), positions.as<float>() + 3 * first, n * 12,
+                               cudaMemcpyDeviceToHost, stream));
+    SERVER_TRY(cudaMemcpyAsync(out.remaining.data(), remaining.as<uint64_t>() + first, n * 8,
+                               cudaMemcpyDeviceToHost, stream));
+    SERVER_TRY(cudaMemcpyAsync(out.termination.data(), termination.as<uint8_t>() + first, n,
+                               cudaMemcpyDeviceToHost, stream));
+  }
+  uint64_t vertex_count = 0, index_count = 0;
+  if (q.record && n) {
+    // Emission of the request's curve, as one round of the reference.
+    SERVER_TRY(raw_counts.reserve(n * 8));
+    SERVER_TRY(wide.reserve(n * 8));
+    SERVER_TRY(vertex_offsets.reserve(n * 8));
+    SERVER_TRY(segment_offsets.reserve(n * 8));
+    SERVER_TRY(dpa::launch_raw_counts(remaining_initial.as<uint64_t>() + first,
+                                      remaining.as<uint64_t>() + first, n,
+                                      raw_counts.as<uint64_t>(), stream));
+    auto scan = [&](const uint32_t* in, uint64_t* out_offsets) {
+      SERVER_TRY(dpa::launch_widen_u32(in, n, wide.as<uint64_t>(), stream));
+      size_t temp = 0;
+      SERVER_TRY(cub::DeviceScan::ExclusiveSum(nullptr, temp, wide.as<uint64_t>(), out_offsets,
+                                               int64_t(n), stream));
+      SERVER_TRY(scan_temp.reserve(temp));
+      SERVER_TRY(cub::DeviceScan::ExclusiveSum(scan_temp.ptr, temp, wide.as<uint64_t>(),
+                                               out_offsets, int64_t(n), stream));
+    };
+    scan(kept_vertices.as<uint32_t>() + first, vertex_offsets.as<uint64_t>());
+    scan(kept_segments.as<uint32_t>() + first, segment_offsets.as<uint64_t>());
+    uint64_t tail[2];
+    uint32_t last[2];
+    SERVER_TRY(cudaMemcpyAsync(&tail[0], vertex_offsets.as<uint64_t>() + (n - 1), 8,
+                               cudaMemcpyDeviceToHost, stream));
+    SERVER_TRY(cudaMemcpyAsync(&tail[1], segment_offsets.as<uint64_t>() + (n - 1), 8,
+                               cudaMemcpyDeviceToHost, stream));
+    SERVER_TRY(cudaMemcpyAsync(&last[0], kept_vertices.as<uint32_t>() + first + (n - 1), 4,
+                               cudaMemcpyDeviceToHost, stream));
+    SERVER_TRY(cudaMemcpyAsync(&last[1], kept_segments.as<uint32_t>() + first + (n - 1), 4,
+                               cudaMemcpyDeviceToHost, stream));
+    SERVER_TRY(cudaStreamSynchronize(stream));
+    vertex_count = tail[0] + last[0];
+    index_count = 2 * (tail[1] + last[1]);
+    const size_t index_bytes = q.index64 ? 8 : 4;
+    SERVER_TRY(out_vertices.reserve(vertex_count * 12));
+    SERVER_TRY(out_colors.reserve(vertex_count * 4));
+    SERVER_TRY(out_indices.reserve(index_count * index_bytes));
+    dpa::EmitArgs e{};
+    e.count = n;
+    e.raw_vertices = raw.as<float>();
+    e.raw_offsets = raw_offsets.as<uint64_t>() + first;
+    e.steps_raw = raw_counts.as<uint64_t>();
+    e.vertex_offsets = vertex_offsets.as<uint64_t>();
+    e.segment_offsets = segment_offsets.as<uint64_t>();
+    e.kept_vertices = kept_vertices.as<uint32_t>() + first;
+    e.vertex_base = 0;
+    e.vertices = out_vertices.as<float>();
+    e.colors = out_colors.as<float>();
+    e.indices = out_indices.ptr;
+    SERVER_TRY(dpa::launch_emit(e, q.index64 != 0, true, stream));
+    out.vertices.resize(3 * vertex_count);
+    out.colors.resize(vertex_count);
+    SERVER_TRY(cudaMemcpyAsync(out.vertices.data(), out_vertices.ptr, vertex_count * 12,
+                               cudaMemcpyDeviceToHost, stream));
+    SERVER_TRY(cudaMemcpyAsync(out.colors.data(), out_colors.ptr, vertex_count * 4,
+                               cudaMemcpyDeviceToHost, stream));
+    if (q.index64) {
+      out.indices64.resize(index_count);
+      SERVER_TRY(cudaMemcpyAsync(out.indices64.data(), out_indices.ptr, index_count * 8,
+                                 cudaMemcpyDeviceToHost, stream));
+    } else {
+      out.indices32.resize(index_count);
+      SERVER_TRY(cudaMemcpyAsync(out.indices32.data(), out_indices.ptr, index_count * 4,
+                                 cudaMemcpyDeviceToHost, stream));
+    }
+  }
+  SERVER_TRY(cudaStreamSynchronize(stream));
+  uint64_t steps = 0;
+  for (uint64_t i = 0; i < n; ++i) steps += q.iterations - out.remaining[i];
+  stats.particle_steps += steps;
+  dpa_response& r = out.r;
+  r.status = DPA_OK;
+  if (q.ftle && n) {
+    // Lattice FTLE of the final positions (ftle_estimator.cpp:7-65); the
+    // seeds should be the lattice of seed_stride on the request's field.
+    const dpa_field* field = fields[size_t(q.field)];
+    dpa::FtleArgs f{};
+    for (int i = 0; i < 3; ++i) {
+      const float stride = q.seed_stride[i] > 0.0f ? q.seed_stride[i] : 1.0f;
+      const float cells = float(field->shape[i]) / stride;
+      f.shape[i] = cells > 0.0f ? uint64_t(cells) : 0;
+      f.offset[i] = field->offset[i];
+      f.spacing[i] = field->spacing[i] * stride;
+      f.two_spacing[i] = 2.0f * f.spacing[i];
+      r.ftle_shape[i] = f.shape[i];
+    }
+    const uint64_t cells = f.shape[0] * f.shape[1] * f.shape[2];
+    if (cells) {
+      SERVER_TRY(ftle_original.reserve(n * 12));
+      SERVER_TRY(ftle_winners.reserve(cells * 8));
+      SERVER_TRY(ftle_flow.reserve(cells * 12));
+      SERVER_TRY(ftle_out.reserve(cells * 4));
+      SERVER_TRY(cudaMemcpyAsync(ftle_original.ptr, a.p.positions.data(), n * 12,
+                                 cudaMemcpyHostToDevice, stream));
+      f.count = n;
+      f.original_positions = ftle_original.as<float>();
+      f.final_positions = positions.as<float>() + 3 * first;
+      f.mapping = DPA_FTLE_MAPPING_REFERENCE;
+      f.horizon = double(std::fabs(q.step_size * float(q.iterations)));
+      f.winners = ftle_winners.as<unsigned long long>();
+      f.flow = ftle_flow.as<float>();
+      f.ftle = ftle_out.as<float>();
+      SERVER_TRY(dpa::launch_ftle(f, stream));
+      out.ftle.resize(cells);
+      SERVER_TRY(cudaMemcpyAsync(out.ftle.data(), ftle_out.ptr, cells * 4, cudaMemcpyDeviceToHost,
+                                 stream));
+      SERVER_TRY(cudaStreamSynchronize(stream));
+    }
+  }
+  r.id = a.p.id;
+  r.user = q.user;
+  r.count = n;
+  r.positions = out.positions.data();
+  r.remaining = out.remaining.data();
+  r.termination = out.termination.data();
+  r.vertex_count = vertex_count;
+  r.vertices = out.vertices.empty() ? nullptr : out.vertices.data();
+  r.colors = out.colors.empty() ? nullptr : out.colors.data();
+  r.index_count = index_count;
+  r.indices = q.index64 ? static_cast<const void*>(out.indices64.data())
+                        : static_cast<const void*>(out.indices32.data());
+  r.ftle = out.ftle.empty() ? nullptr : out.ftle.data();
+  r.particle_steps = steps;
+  r.queued_seconds = a.p.queued;
+  r.admitted_seconds = a.admitted;
+  r.finished_seconds = now();
+}
+
+void dpa_server::run() {
+  try {
+    SERVER_TRY(cudaSetDevice(ctx->device));
+    while (true) {
+      std::vector<active_request> admitted;
+      {
+        std::unique_lock<std::mutex> lock(mutex);
+        select(admitted);
+        if (active.empty() && admitted.empty()) {
+          if (stopping && queue.empty()) break;
+          wake.wait_for(lock, std::chrono::milliseconds(2));
+          continue;
+        }
+      }
+      for (const active_request& a : admitted) upload(a);
+      {
+        std::lock_guard<std::mutex> lock(mutex);
+        for (active_request& a : admitted) active.push_back(std::move(a));
+        stats.admitted += admitted.size();
+      }
+      const auto t0 = clock_type::now();
+      tick();
+      // Which requests have no particle in flight any more?
+      SERVER_TRY(host_in_flight.reserve(4 * uint64_t(options.max_requests)));
+      SERVER_TRY(cudaMemcpyAsync(host_in_flight.ptr, in_flight.ptr, 4 * uint64_t(options.max_requests),
+                                 cudaMemcpyDeviceToHost, stream));
+      SERVER_TRY(cudaStreamSynchronize(stream));
+      const unsigned int* left = host_in_flight.as<unsigned int>();
+      std::vector<std::unique_ptr<response_storage>> finished;
+      std::vector<size_t> finished_at;
+      for (size_t i = 0; i < active.size(); ++i) {
+        if (left[active[i].slot] != 0) continue;
+        auto out = std::make_unique<response_storage>();
+        finish(active[i], *out);
+        finished.push_back(std::move(out));
+        finished_at.push_back(i);
+      }
+      stats.busy_seconds += std::chrono::duration<double>(clock_type::now() - t0).count();
+      std::lock_guard<std::mutex> lock(mutex);
+      for (size_t j = finished_at.size(); j-- > 0;) {
+        active_request& a = active[finished_at[j]];
+        slots.release(a.first, a.p.request.count);
+        vertices.release(a.raw_first, a.raw_count);
+        free_counters.push_back(a.slot);
+        active.erase(active.begin() + long(finished_at[j]));
+      }
+      for (auto& out : finished) {
+        const uint64_t id = out->r.id;
+        done_order.push_back(id);
+        done[id] = std::move(out);
+        stats.completed += 1;
+      }
+      if (!finished.empty()) done_signal.notify_all();
+    }
+  } catch (const std::exception& e) {
+    std::lock_guard<std::mutex> lock(mutex);
+    failure = e.what();
+    stopping = true;
+    done_signal.notify_all();
+  }
+}
+
+extern "C" {
+
+int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_server** out) {
+  if (!ctx || !options || !out) return DPA_ERROR_INVALID_ARGUMENT;
+  *out = nullptr;
+  if (options->particle_capacity == 0 || options->max_requests == 0) {
+    ctx->error = "server needs particle_capacity and max_requests";
+    return DPA_ERROR_INVALID_ARGUMENT;
+  }
+  try {
+    auto s = std::make_unique<dpa_server>();
+    s->ctx = ctx;
+    s->options = *options;
+    if (cudaSetDevice(ctx->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+      ctx->error = "server: cannot create a stream";
+      return DPA_ERROR_CUDA;
+    }
+    const uint64_t p = options->particle_capacity, v = options->vertex_capacity;
+    cudaError_t e = cudaSuccess;
+    DeviceBuffer* per_slot[] = {&s->positions, &s->remaining, &s->remaining_initial,
+                                &s->termination, &s->raw_offsets, &s->kept_vertices,
+                                &s->kept_segments, &s->curve_open, &s->request_of};
+    const size_t bytes[] = {12, 8, 8, 1, 8, 4, 4, 1, 4};
+    for (size_t i = 0; i < 9 && e == cudaSuccess; ++i) e = per_slot[i]->reserve(p * bytes[i]);
+    if (e == cudaSuccess) e = s->raw.reserve(std::max<uint64_t>(v, 1) * 12);
+    if (e == cudaSuccess) e = s->in_flight.reserve(4 * uint64_t(options->max_requests));
+    if (e == cudaSuccess) e = s->work_counter.reserve(8);
+    if (e == cudaSuccess)
+      e = cudaMemsetAsync(s->in_flight.ptr, 0, 4 * uint64_t(options->max_requests), s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) {
+      cudaStreamDestroy(s->stream);
+      ctx->error = std::string("server: device arenas: ") + cudaGetErrorName(e);
+      return e == cudaErrorMemoryAllocation ? DPA_ERROR_OUT_OF_MEMORY : DPA_ERROR_CUDA;
+    }
+    s->slots.reset(p);
+    s->vertices.reset(v);
+    for (uint32_t i = options->max_requests; i-- > 0;) s->free_counters.push_back(i);
+    dpa_server* raw_ptr = s.get();
+    s->worker = std::thread([raw_ptr] { raw_ptr->run(); });
+    *out = s.release();
+    return DPA_OK;
+  } catch (const std::exception& e) {
+    ctx->error = e.what();
+    return DPA_ERROR_INTERNAL;
+  }
+}
+
+int dpa_server_add_field(dpa_server* s, const dpa_field* field, int32_t* id) {
+  if (!s || !field || !id || field->owner != s->ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(s->mutex);
+  s->fields.push_back(field);
+  *id = int32_t(s->fields.size() - 1);
+  return DPA_OK;
+}
+
+int dpa_server_submit(dpa_server* s, const dpa_request* request, uint64_t* id) {
+  if (!s || !request || !id) return DPA_ERROR_INVALID_ARGUMENT;
+  const dpa_request& q = *request;
+  {
+    std::lock_guard<std::mutex> lock(s->mutex);
+    if (q.field < 0 || size_t(q.field) >= s->fields.size()) return DPA_ERROR_INVALID_ARGUMENT;
+  }
+  if (!integrator_ok(q.integrator)) return DPA_ERROR_UNSUPPORTED;
+  if (q.count && !q.positions) return DPA_ERROR_INVALID_ARGUMENT;
+  if (q.count > s->options.particle_capacity) return DPA_ERROR_OUT_OF_MEMORY;
+  if (q.record && q.count * (q.iterations + 2) > s->options.vertex_capacity)
+    return DPA_ERROR_OUT_OF_MEMORY;
+  if (q.record && q.iterations > 0xfffffff0ull) return DPA_ERROR_INVALID_ARGUMENT;
+  if (q.count > 0xffffffffull) return DPA_ERROR_INVALID_ARGUMENT;
+  try {
+    pending p;
+    p.request = q;
+    p.positions.assign(q.positions, q.positions + 3 * q.count);
+    std::lock_guard<std::mutex> lock(s->mutex);
+    if (!s->failure.empty() || s->stopping) return DPA_ERROR_INTERNAL;
+    p.id = s->next_id++;
+    p.queued = s->now();
+    *id = p.id;
+    s->queue.push_back(std::move(p));
+    s->stats.submitted += 1;
+  } catch (const std::bad_alloc&) {
+    return DPA_ERROR_OUT_OF_MEMORY;
+  }
+  s->wake.notify_one();
+  return DPA_OK;
+}
+
+int dpa_server_poll(dpa_server* s, int32_t wait_ms, dpa_response* out, int32_t* got) {
+  if (!s || !out || !got) return DPA_ERROR_INVALID_ARGUMENT;
+  *got = 0;
+  std::unique_lock<std::mutex> lock(s->mutex);
+  const auto ready = [&] { return !s->done_order.empty() || !s->failure.empty(); };
+  if (wait_ms > 0) s->done_signal.wait_for(lock, std::chrono::milliseconds(wait_ms), ready);
+  if (s->done_order.empty()) {
+    if (!s->failure.empty()) {
+      s->ctx->error = "server: " + s->failure;
+      return DPA_ERROR_CUDA;
+    }
+    return DPA_OK;
+  }
+  const uint64_t id = s->done_order.front();
+  s->done_order.pop_front();
+  auto it = s->done.find(id);
+  *out = it->second->r;
+  s->handed_out[id] = std::move(it->second);
+  s->done.erase(it);
+  *got = 1;
+  return DPA_OK;
+}
+
+int dpa_server_release(dpa_server* s, uint64_t id) {
+  if (!s) return DPA_ERROR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(s->mutex);
+  return s->handed_out.erase(id) ? DPA_OK : DPA_ERROR_INVALID_ARGUMENT;
+}
+
+int dpa_server_get_stats(dpa_server* s, dpa_server_stats* out) {
+  if (!s || !out) return DPA_ERROR_INVALID_ARGUMENT;
+  std::lock_guard<std::mutex> lock(s->mutex);
+  *out = s->stats;
+  out->queued = uint32_t(s->queue.size());
+  out->active = uint32_t(s->active.size());
+  return DPA_OK;
+}
+
+int dpa_server_destroy(dpa_server* s) {
+  if (!s) return DPA_ERROR_INVALID_ARGUMENT;
+  {
+    std::lock_guard<std::mutex> lock(s->mutex);
+    s->stopping = true;
+  }
+  s->wake.notify_all();
+  if (s->worker.joinable()) s->worker.join();
+  cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->stream);
+  cudaStreamDestroy(s->stream);
+  delete s;
+  return DPA_OK;
+}
+
+}  // extern "C"

@@ -27,6 +27,8 @@ extern "C" {
 
 typedef struct dpa_context dpa_context;
 typedef struct dpa_field dpa_field;
+typedef struct dpa_graph dpa_graph;
+typedef struct dpa_server dpa_server;
 
 typedef enum dpa_status {
   DPA_OK = 0,
@@ -70,7 +72,8 @@ typedef enum dpa_integrator {
 typedef enum dpa_termination {
   DPA_TERMINATION_COMPLETE = 0,      /* remaining_iterations reached 0 */
   DPA_TERMINATION_OUT_OF_BOUNDS = 1, /* regular_grid::contains failed */
-  DPA_TERMINATION_ZERO_VELOCITY = 2  /* interpolated vector isZero() */
+  DPA_TERMINATION_ZERO_VELOCITY = 2, /* interpolated vector isZero() */
+  DPA_TERMINATION_IN_FLIGHT = 3      /* stopped by dpa_advect_options.max_steps; resumable */
 } dpa_termination;
 
 /* FTLE scatter rule. REFERENCE puts each final position into the flow-map
@@ -90,6 +93,11 @@ typedef struct dpa_advect_options {
   int32_t index64;      /* 64-bit indices (pipeline.cpp:155 decides) */
   int32_t colors;       /* emit angular-velocity colors with the curve */
   int32_t morton_order; /* process particles in Morton order of their start cell */
+  uint64_t max_steps;   /* 0: no limit. Otherwise a particle takes at most this
+                           many steps per call and, if it could go on, ends the
+                           call as DPA_TERMINATION_IN_FLIGHT with its position
+                           and remaining count updated, ready to resume (device
+                           calls without recording only) */
 } dpa_advect_options;
 
 /* One piece of a round's curve, delivered in order. The round's curve is the
@@ -190,6 +198,130 @@ int dpa_advect_round(dpa_context* ctx, const dpa_field* field, const dpa_advect_
 int dpa_advect_device(dpa_context* ctx, const dpa_field* field, const dpa_advect_options* options,
                       uint64_t count, float* device_positions, uint64_t* device_remaining,
                       uint8_t* device_termination, void* stream);
+
+/* ---- batching, graphs and tuning (no counterpart in the reference) -------- */
+
+/* Many seed sets in one persistent launch: set s is particles
+ * [set_offsets[s], set_offsets[s+1]) of the device arrays (set_offsets is a
+ * host array of set_count + 1 entries starting at 0). Every particle carries
+ * its own remaining count, so sets of any size and iteration count share the
+ * launch. set_steps (host, may be NULL) receives the particle-steps each set
+ * took; asking for it makes the call wait for the launch. No recording. */
+int dpa_advect_batch_device(dpa_context* ctx, const dpa_field* field,
+                            const dpa_advect_options* options, uint64_t set_count,
+                            const uint64_t* set_offsets, float* device_positions,
+                            uint64_t* device_remaining, uint8_t* device_termination,
+                            uint64_t* set_steps, void* stream);
+
+/* The launch sequence of dpa_advect_device (processing order + advection) for
+ * fixed device arrays, captured once into a CUDA graph; each
+ * dpa_graph_launch replays it on a stream (NULL: the context's). The graph
+ * shares the context's scratch: launch it on one stream at a time. */
+int dpa_graph_create_advect(dpa_context* ctx, const dpa_field* field,
+                            const dpa_advect_options* options, uint64_t count,
+                            float* device_positions, uint64_t* device_remaining,
+                            uint8_t* device_termination, dpa_graph** out);
+int dpa_graph_launch(dpa_context* ctx, dpa_graph* graph, void* stream);
+int dpa_graph_destroy(dpa_context* ctx, dpa_graph* graph);
+
+/* Launch parameters of a context's advection kernels. */
+typedef struct dpa_tuning {
+  uint32_t claim;          /* processing-order entries a warp takes per atomic claim */
+  uint32_t blocks_per_sm;  /* persistent grid blocks per SM; 0 = as many as fit */
+  uint32_t order;          /* processing order: Morton buckets of a order^3 coarsening
+                              of the grid (1..16), 0 = input order */
+  float    measured_ms;    /* dpa_autotune_advect: time of the chosen setting */
+} dpa_tuning;
+
+int dpa_context_set_tuning(dpa_context* ctx, const dpa_tuning* tuning);
+int dpa_context_get_tuning(const dpa_context* ctx, dpa_tuning* tuning);
+
+/* Times the candidate settings (claim 16..128, 2 to all resident blocks per SM,
+ * order 16 / 8 / off) on a sample of up to 262,144 of the given device
+ * particles, each advanced at most sample_steps steps (0: 200) on copies,
+ * keeps the fastest in the context and returns it in best (may be NULL). */
+int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_advect_options* options,
+                        uint64_t count, const float* device_positions,
+                        const uint64_t* device_remaining, uint64_t sample_steps,
+                        dpa_tuning* best);
+
+/* ---- serving (no counterpart in the reference) ------------------------------ */
+
+/* A request server: fields stay resident, requests are admitted first in,
+ * first out when the device arenas have room for them (count particle slots;
+ * for recording requests also count * (iterations + 2) curve-staging
+ * vertices, their output buffer), and admitted requests advance together in
+ * ticks of steps_per_tick steps: one persistent launch per group of requests
+ * sharing a field, integrator, step size and recording switch. Requests that
+ * arrive while others run join at the next tick. A worker thread owns the
+ * device work; submit, poll and stats may be called from any thread. The
+ * context is used for its device and its fields only. */
+typedef struct dpa_server_options {
+  uint64_t particle_capacity;  /* particle slots of the arena */
+  uint64_t vertex_capacity;    /* curve-staging vertices of the arena (12 bytes each) */
+  uint32_t steps_per_tick;     /* step budget of each tick (0: 64) */
+  uint32_t max_requests;       /* requests admitted at once */
+} dpa_server_options;
+
+typedef struct dpa_request {
+  int32_t     field;           /* from dpa_server_add_field */
+  int32_t     integrator;      /* dpa_integrator */
+  float       step_size;
+  int32_t     record;          /* return the curve (pruned, indexed, colored) */
+  int32_t     index64;
+  int32_t     ftle;            /* also return the lattice FTLE of the final positions */
+  float       seed_stride[3];  /* FTLE: the seeds' lattice stride in cells */
+  uint64_t    count;
+  const float* positions;      /* host, count * 3; copied by dpa_server_submit */
+  uint64_t    iterations;      /* per seed */
+  void*       user;
+} dpa_request;
+
+/* A finished request. Arrays are host memory owned by the server until
+ * dpa_server_release(id). Times are seconds since the server started. */
+typedef struct dpa_response {
+  uint64_t       id;
+  void*          user;
+  int32_t        status;
+  uint64_t       count;
+  const float*   positions;
+  const uint64_t* remaining;
+  const uint8_t* termination;
+  uint64_t       vertex_count;
+  const float*   vertices;
+  const float*   colors;
+  uint64_t       index_count;
+  const void*    indices;       /* uint32 or uint64 per the request's index64 */
+  uint64_t       ftle_shape[3];
+  const float*   ftle;
+  uint64_t       particle_steps;
+  double         queued_seconds;
+  double         admitted_seconds;
+  double         finished_seconds;
+} dpa_response;
+
+typedef struct dpa_server_stats {
+  uint64_t submitted;
+  uint64_t admitted;
+  uint64_t completed;
+  uint64_t ticks;
+  uint64_t launches;
+  uint64_t particle_steps;
+  double   busy_seconds;
+  uint32_t queued;
+  uint32_t active;
+} dpa_server_stats;
+
+int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_server** out);
+int dpa_server_add_field(dpa_server* server, const dpa_field* field, int32_t* field_id);
+/* Queues a request; DPA_ERROR_OUT_OF_MEMORY when it could never fit the arenas. */
+int dpa_server_submit(dpa_server* server, const dpa_request* request, uint64_t* id);
+/* Takes one finished request (*got = 1), waiting up to wait_ms for one. */
+int dpa_server_poll(dpa_server* server, int32_t wait_ms, dpa_response* out, int32_t* got);
+int dpa_server_release(dpa_server* server, uint64_t id);
+int dpa_server_get_stats(dpa_server* server, dpa_server_stats* out);
+/* Finishes the admitted and queued requests, then stops the worker. */
+int dpa_server_destroy(dpa_server* server);
 
 /* ---- allocation-free advection ----------------------------------------------- */
 

@@ -1,0 +1,121 @@
+"""The request server: every result is the same alone and in a mix of
+concurrent requests (bit for bit), requests that do not fit wait for room,
+and requests that can never fit are refused."""
+import math
+
+import numpy as np
+import pytest
+
+import dpa_b200
+from dpa_b200 import ParticleAdvector, Particles, fields, seeds
+from dpa_b200.serve import Server
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def resident(ctx):
+    abc = fields.abc(48)
+    noise = fields.curl_noise(64, 4.0, 8)
+    f_abc = ctx.field(abc)
+    f_noise = ctx.field(noise)
+    yield {"abc": (abc, f_abc), "noise": (noise, f_noise)}
+    f_abc.close()
+    f_noise.close()
+
+
+def alone(ctx, field, positions, iterations, integrator, step, record):
+    adv = ParticleAdvector(ctx, max(len(positions), 1), "none", integrator, step, False, record,
+                           use_64_bit_indices=False)
+    return adv.advect(field, Particles.create(positions, iterations))
+
+
+def make_requests(resident):
+    rng = np.random.default_rng(11)
+    reqs = []
+    for i in range(14):
+        name = "abc" if i % 2 else "noise"
+        grid, field = resident[name]
+        offset, size = seeds.seed_box(grid)
+        count = int(rng.integers(50, 6000))
+        iters = int(rng.integers(20, 300))
+        step = 0.02 if name == "abc" else 0.25
+        record = bool(i % 3 == 0)
+        integ = ["runge_kutta_4", "euler", "runge_kutta_4"][i % 3]
+        pos = seeds.generate_random(offset, size, count, iters, seed=100 + i).position
+        reqs.append(dict(name=name, positions=pos, iterations=iters, step=step, record=record,
+                         integrator=integ))
+    return reqs
+
+
+def test_results_are_the_same_alone_and_in_the_mix(ctx, resident):
+    reqs = make_requests(resident)
+    with Server(ctx, particle_capacity=40000, vertex_capacity=4_000_000, steps_per_tick=32,
+                max_requests=64) as server:
+        ids = {}
+        fid = {name: server.add_field(f) for name, (_, f) in resident.items()}
+        for r in reqs:
+            rid = server.submit(fid[r["name"]], r["positions"], r["iterations"], r["integrator"],
+                                r["step"], r["record"])
+            ids[rid] = r
+        results = {}
+        while len(results) < len(reqs):
+            res = server.poll(wait_ms=2000)
+            assert res is not None, server.stats()
+            results[res.id] = res
+        stats = server.stats()
+    assert stats["completed"] == len(reqs) and stats["ticks"] > 1
+    for rid, r in ids.items():
+        res = results[rid]
+        assert res.status == 0
+        want = alone(ctx, resident[r["name"]][1], r["positions"], r["iterations"],
+                     r["integrator"], r["step"], r["record"])
+        np.testing.assert_array_equal(res.positions, want.inactive_particles.position)
+        np.testing.assert_array_equal(res.termination, want.inactive_particles.termination)
+        np.testing.assert_array_equal(res.remaining, want.inactive_particles.remaining_iterations)
+        if r["record"]:
+            curve = want.integral_curves[0]
+            np.testing.assert_array_equal(res.vertices, curve.vertices)
+            np.testing.assert_array_equal(res.indices, curve.indices)
+            np.testing.assert_array_equal(res.colors, curve.colors)
+        assert res.queued <= res.admitted <= res.finished
+
+
+def test_ftle_request_matches_the_stage_api(ctx, resident):
+    grid, field = resident["abc"]
+    offset, size = seeds.seed_box(grid)
+    stride = (grid.spacing * np.float32(2)).astype(np.float32)
+    lattice = seeds.generate(offset, size, stride, 30)
+    with Server(ctx, particle_capacity=20000, steps_per_tick=16, max_requests=4) as server:
+        fid = server.add_field(field)
+        server.submit(fid, lattice.position, 30, step_size=0.02, ftle=True,
+                      seed_stride=(2, 2, 2))
+        res = server.poll(wait_ms=5000)
+    assert res is not None and res.status == 0
+    out = alone(ctx, field, lattice.position, 30, "runge_kutta_4", 0.02, False)
+    want = dpa_b200.estimate_ftle(ctx, field, 30, (2, 2, 2), 0.02, out.inactive_particles)
+    np.testing.assert_array_equal(res.ftle, want.data)
+
+
+def test_admission_waits_for_room_and_refuses_what_never_fits(ctx, resident):
+    grid, field = resident["noise"]
+    offset, size = seeds.seed_box(grid)
+    with Server(ctx, particle_capacity=5000, vertex_capacity=100_000, steps_per_tick=64,
+                max_requests=2) as server:
+        fid = server.add_field(field)
+        with pytest.raises(dpa_b200.DpaError) as e:
+            server.submit(fid, np.zeros((6000, 3), np.float32), 10)
+        assert e.value.status == 3
+        with pytest.raises(dpa_b200.DpaError):
+            server.submit(fid, np.zeros((1000, 3), np.float32), 200, record=True)
+        ids = [server.submit(fid, seeds.generate_random(offset, size, 3000, 50, seed=s).position,
+                             50) for s in range(5)]
+        got = []
+        while len(got) < 5:
+            res = server.poll(wait_ms=5000)
+            assert res is not None
+            got.append(res)
+    assert sorted(r.id for r in got) == sorted(ids)
+    # 3000-particle requests in a 5000-slot arena run one at a time, in order.
+    order = [r.id for r in sorted(got, key=lambda r: r.admitted)]
+    assert order == sorted(ids)
