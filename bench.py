@@ -54,6 +54,10 @@ def parse_args():
     p.add_argument("--step-size", type=float, default=0.25)
     p.add_argument("--cpu-seconds", type=float, default=10.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-systems", action="store_true",
+                   help="skip the batched / graph / serving measurements")
+    p.add_argument("--serve-seconds", type=float, default=10.0)
+    p.add_argument("--batch-n", type=int, default=512)
     return p.parse_args()
 
 
@@ -232,6 +236,206 @@ def precision_forms(a, ctx, grid, parts, p0, r0, pos, rem, term, stream, f32_ker
                         "fp64_error": fp64_error(a, ctx, field, grid, parts, horizons=(50, 250))}
         field.close()
     return out
+
+
+def _graph_replays(ctx, field, opts, p0, r0, pos, rem, term, stream, steps):
+    """Times `steps` replays of the captured order + advection graph, each
+    after a device reset of the particle state; returns mean ms per replay."""
+    import ctypes as C
+    import torch
+    lib = ctx._lib
+    graph = C.c_void_p()
+    n = p0.shape[0]
+    ctx.check(lib.dpa_graph_create_advect(ctx.handle, field.handle, C.byref(opts), n,
+                                          C.c_void_p(pos.data_ptr()), C.c_void_p(rem.data_ptr()),
+                                          C.c_void_p(term.data_ptr()), C.byref(graph)))
+    times = []
+    try:
+        for i in range(steps + 2):
+            start = torch.cuda.Event(enable_timing=True)
+            end = torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            pos.copy_(p0)
+            rem.copy_(r0)
+            ctx.check(lib.dpa_graph_launch(ctx.handle, graph, C.c_void_p(stream.cuda_stream)))
+            end.record(stream)
+            end.synchronize()
+            if i >= 2:
+                times.append(start.elapsed_time(end))
+    finally:
+        lib.dpa_graph_destroy(ctx.handle, graph)
+    return statistics.mean(times)
+
+
+def systems_forms(a, ctx, grid, p0, r0, pos, rem, term, stream, plain_ms, steps=10):
+    """The batched form on the same workload: field in FP16 (and FP32 for
+    comparison), launch parameters autotuned on a sample, the order +
+    advection sequence replayed from a CUDA graph. Ratios are against this
+    run's plain FP32 step (dpa_advect_device, default parameters)."""
+    import ctypes as C
+    from dpa_b200 import _native as N
+    lib = ctx._lib
+    out = {}
+    saved = N.Tuning()
+    ctx.check(lib.dpa_context_get_tuning(ctx.handle, C.byref(saved)))
+    for storage in ("f16", "f32"):
+        field = ctx.field(grid, storage)
+        opts = N.AdvectOptions(N.INTEGRATORS[a.integrator], float(np.float32(a.step_size)),
+                               0, 0, 0, 1, 0)
+        best = N.Tuning()
+        ctx.check(lib.dpa_autotune_advect(ctx.handle, field.handle, C.byref(opts), a.seeds,
+                                          C.c_void_p(p0.data_ptr()), C.c_void_p(r0.data_ptr()),
+                                          200, C.byref(best)))
+        ms = _graph_replays(ctx, field, opts, p0, r0, pos, rem, term, stream, steps)
+        taken = float((a.iterations - rem.cpu().numpy().astype(np.int64)).sum())
+        out[f"{storage}_autotuned_graph"] = {
+            "ms_per_step": ms, "particle_steps_per_s": taken / (ms / 1e3),
+            "speedup_vs_plain_f32": plain_ms / ms,
+            "tuning": {"claim": best.claim, "blocks_per_sm": best.blocks_per_sm,
+                       "order": best.order}}
+        ctx.check(lib.dpa_context_set_tuning(ctx.handle, C.byref(saved)))
+        field.close()
+    return out
+
+
+def batched_run(a, ctx, stream, sets=64):
+    """Many seed sets in one persistent launch: a curl-noise field of
+    batch_n^3 (sigma 8, seed 3), 64 seed sets with log-uniform sizes in
+    [1e3, 1e6] (scaled to the grid when batch_n < 512) and iterations uniform
+    in [200, 4000], RK4 step 0.25, end positions only (recording 16 M curves
+    of up to 4000 vertices would be ~0.8 TB of output)."""
+    import ctypes as C
+    import torch
+    from dpa_b200 import _native as N
+    from dpa_b200 import fields, seeds
+    lib = ctx._lib
+    n = a.batch_n
+    grid = fields.curl_noise(n, 8.0, 3, device="cuda")
+    torch.cuda.empty_cache()
+    rng = np.random.default_rng(3)
+    scale = (n / 512.0) ** 3
+    sizes = np.exp(rng.uniform(np.log(1e3), np.log(1e6), size=sets)) * scale
+    sizes = np.maximum(sizes.astype(np.int64), 1)
+    iters = rng.integers(200, 4001, size=sets)
+    offset, size = seeds.seed_box(grid)
+    box = ([0.0] * 3, [float(n - 1)] * 3)
+    total = int(sizes.sum())
+    pos_h = seeds.generate_random(offset, size, total, 0, aabb=box, seed=3).position
+    rem_h = np.repeat(iters, sizes).astype(np.int64)
+    set_offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    out = {"grid": n, "sets": sets, "particles": total,
+           "iterations": {"min": int(iters.min()), "max": int(iters.max())}}
+    p0 = torch.from_numpy(pos_h).cuda()
+    r0 = torch.from_numpy(rem_h).cuda()
+    pos = torch.empty_like(p0)
+    rem = torch.empty_like(r0)
+    term = torch.empty(total, dtype=torch.uint8, device="cuda")
+    for storage in ("f32", "f16"):
+        field = ctx.field(grid, storage)
+        opts = N.AdvectOptions(N.INTEGRATORS[a.integrator], float(np.float32(a.step_size)),
+                               0, 0, 0, 1, 0)
+        set_steps = np.zeros(sets, np.uint64)
+        times = []
+        for i in range(3):
+            pos.copy_(p0)
+            rem.copy_(r0)
+            start = torch.cuda.Event(enable_timing=True)
+            end = torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            ctx.check(lib.dpa_advect_batch_device(
+                ctx.handle, field.handle, C.byref(opts), sets,
+                set_offsets.ctypes.data_as(N._U64P), C.c_void_p(pos.data_ptr()),
+                C.c_void_p(rem.data_ptr()), C.c_void_p(term.data_ptr()),
+                set_steps.ctypes.data_as(N._U64P) if i == 0 else None,
+                C.c_void_p(stream.cuda_stream)))
+            end.record(stream)
+            end.synchronize()
+            if i > 0:
+                times.append(start.elapsed_time(end))
+        ms = statistics.mean(times)
+        steps_total = float(set_steps.sum())
+        out[storage] = {"ms_per_batch": ms, "particle_steps": steps_total,
+                        "particle_steps_per_s": steps_total / (ms / 1e3),
+                        "field_device_bytes": field.device_bytes}
+        field.close()
+    del p0, r0, pos, rem, term
+    torch.cuda.empty_cache()
+    return out
+
+
+def serving_run(a, ctx, rate=200.0):
+    """Poisson arrivals (seed 4) at `rate` requests/s for serve_seconds on a
+    resident 256^3 curl-noise field. Request mix: 10 % FTLE on a 64^3
+    lattice; 50 % recording, seeds log-uniform in [1e2, 2e3] (the returned
+    curves must fit host memory and the link); 40 % end positions, seeds
+    log-uniform in [1e2, 1e6]; iterations uniform in [100, 5000]. Seeds are
+    windows of a pre-drawn pool so that submitting keeps pace with the
+    arrivals. Latency is submit to result; throughput counts particle-steps
+    over the wall time of the run."""
+    import threading as th
+    from dpa_b200 import fields, seeds
+    from dpa_b200.serve import Server
+    grid = fields.curl_noise(256, 4.0, 1, device="cuda")
+    field = ctx.field(grid, "f32")
+    rng = np.random.default_rng(4)
+    offset, size = seeds.seed_box(grid)
+    pool = seeds.generate_random(offset, size, 2_000_000, 0, aabb=([0.0] * 3, [255.0] * 3),
+                                 seed=4).position
+    lattice = seeds.generate(offset, size, grid.spacing * np.float32(4), 0).position
+    plan = []
+    t = 0.0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > a.serve_seconds:
+            break
+        kind = rng.random()
+        iters = int(rng.integers(100, 5001))
+        if kind < 0.1:
+            plan.append((t, lattice, iters, False, True))
+            continue
+        record = kind < 0.6
+        hi = 2e3 if record else 1e6
+        count = int(np.exp(rng.uniform(np.log(1e2), np.log(hi))))
+        start = int(rng.integers(0, len(pool) - count))
+        plan.append((t, pool[start:start + count], iters, record, False))
+    results = []
+    with Server(ctx, particle_capacity=12_000_000, vertex_capacity=600_000_000,
+                steps_per_tick=64, max_requests=1024) as server:
+        fid = server.add_field(field)
+        done = th.Event()
+
+        def collect():
+            while len(results) < len(plan):
+                r = server.poll(wait_ms=50)
+                if r is not None:
+                    results.append(r)
+                elif done.is_set() and server.stats()["completed"] >= len(plan) and \
+                        len(results) >= len(plan):
+                    break
+        poller = th.Thread(target=collect, daemon=True)
+        poller.start()
+        t0 = time.perf_counter()
+        for when, pos, iters, record, ftle in plan:
+            delay = when - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            server.submit(fid, pos, iters, a.integrator, a.step_size, record=record, ftle=ftle,
+                          seed_stride=(4.0, 4.0, 4.0))
+        done.set()
+        poller.join(timeout=600)
+        wall = time.perf_counter() - t0
+        stats = server.stats()
+    field.close()
+    lat = np.array([r.latency for r in results]) * 1e3
+    steps = float(sum(r.particle_steps for r in results))
+    kinds = {"ftle": sum(1 for p in plan if p[4]), "recording": sum(1 for p in plan if p[3])}
+    return {"requests": len(plan), "completed": len(results), "rate_per_s": rate,
+            "seconds_of_arrivals": a.serve_seconds, "wall_seconds": wall,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)),
+                           "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+            "particle_steps_per_s": steps / wall, "ticks": int(stats["ticks"]),
+            "launches": int(stats["launches"]), "busy_seconds": float(stats["busy_seconds"]),
+            "mix": kinds}
 
 
 def run_reference(a):
@@ -424,6 +628,11 @@ def run_gpu(a):
         out["fp64_error"] = fp64_error(a, ctx, field, grid, parts)
         out["precision_forms"] = precision_forms(a, ctx, grid, parts, pristine_pos, pristine_rem,
                                                  pos, rem, term, stream, statistics.mean(kernel_ms))
+        if not a.no_systems:
+            out["systems_forms"] = systems_forms(a, ctx, grid, pristine_pos, pristine_rem, pos, rem,
+                                                 term, stream, ms_max)
+            out["batched"] = batched_run(a, ctx, stream)
+            out["serving"] = serving_run(a, ctx)
     if rank == 0:
         print(json.dumps(out), flush=True)
     field.close()
