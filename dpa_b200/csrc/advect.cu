@@ -71,7 +71,10 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
       const uint32_t left = uint32_t(claim_end - claim_next);
       const uint32_t take = uint32_t(__popc(idle)) < left ? uint32_t(__popc(idle)) : left;
       const uint32_t rank = __popc(idle & lanes_below);
-      const bool took = !active && rank < take;  // takes entry claim_next + rank
+      // Lanes still in the idle set take entries claim_next + rank. (A lane
+      // that drew a finished particle earlier in this round is inactive but
+      // no longer idle, and must not take one again.)
+      const bool took = ((idle >> lane) & 1u) && rank < take;
       bool mine = took;
       if (mine) {
         const uint64_t t = claim_next + rank;

@@ -2,6 +2,7 @@
 concurrent requests (bit for bit), requests that do not fit wait for room,
 and requests that can never fit are refused."""
 import math
+import time
 
 import numpy as np
 import pytest
@@ -119,3 +120,41 @@ def test_admission_waits_for_room_and_refuses_what_never_fits(ctx, resident):
     # 3000-particle requests in a 5000-slot arena run one at a time, in order.
     order = [r.id for r in sorted(got, key=lambda r: r.admitted)]
     assert order == sorted(ids)
+
+
+@pytest.mark.timeout(300)
+def test_many_concurrent_requests_all_complete(ctx, resident):
+    # Many requests whose particles leave the grid at very different steps,
+    # small ticks: every request must complete, with its counter exact.
+    grid, field = resident["noise"]
+    offset, size = seeds.seed_box(grid)
+    pool = seeds.generate_random(offset, size, 200_000, 0, seed=77).position
+    rng = np.random.default_rng(5)
+    plan = []
+    for i in range(80):
+        count = int(np.exp(rng.uniform(np.log(50), np.log(50_000))))
+        start = int(rng.integers(0, len(pool) - count))
+        plan.append((pool[start:start + count], int(rng.integers(10, 800)), bool(i % 4 == 0)))
+    with Server(ctx, particle_capacity=600_000, vertex_capacity=30_000_000, steps_per_tick=16,
+                max_requests=32) as server:
+        fid = server.add_field(field)
+        ids = {}
+        for pos, iters, record in plan:
+            if record and len(pos) * (iters + 2) > 30_000_000:
+                record = False
+            ids[server.submit(fid, pos, iters, record=record)] = (pos, iters, record)
+        got = {}
+        deadline = time.time() + 240
+        while len(got) < len(plan) and time.time() < deadline:
+            r = server.poll(wait_ms=100)
+            if r is not None:
+                got[r.id] = r
+        stats = server.stats()
+    assert len(got) == len(plan), stats
+    for rid in list(ids)[:10]:
+        pos, iters, record = ids[rid]
+        want = alone(ctx, field, pos, iters, "runge_kutta_4", 0.25, record)
+        np.testing.assert_array_equal(got[rid].positions, want.inactive_particles.position)
+        np.testing.assert_array_equal(got[rid].termination, want.inactive_particles.termination)
+        assert got[rid].particle_steps == int(
+            (iters - want.inactive_particles.remaining_iterations.astype(np.int64)).sum())
