@@ -269,7 +269,7 @@ def _graph_replays(ctx, field, opts, p0, r0, pos, rem, term, stream, steps):
 
 def systems_forms(a, ctx, grid, p0, r0, pos, rem, term, stream, plain_ms, steps=10):
     """The batched form on the same workload: field in FP16 (and FP32 for
-    comparison), launch parameters autotuned on a sample, the order +
+    comparison), launch parameters autotuned on the same seeds and budgets, the order +
     advection sequence replayed from a CUDA graph. Ratios are against this
     run's plain FP32 step (dpa_advect_device, default parameters)."""
     import ctypes as C
@@ -285,7 +285,7 @@ def systems_forms(a, ctx, grid, p0, r0, pos, rem, term, stream, plain_ms, steps=
         best = N.Tuning()
         ctx.check(lib.dpa_autotune_advect(ctx.handle, field.handle, C.byref(opts), a.seeds,
                                           C.c_void_p(p0.data_ptr()), C.c_void_p(r0.data_ptr()),
-                                          200, C.byref(best)))
+                                          0, C.byref(best)))
         ms = _graph_replays(ctx, field, opts, p0, r0, pos, rem, term, stream, steps)
         taken = float((a.iterations - rem.cpu().numpy().astype(np.int64)).sum())
         out[f"{storage}_autotuned_graph"] = {

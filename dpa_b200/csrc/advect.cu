@@ -52,6 +52,7 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
   float* curve = nullptr;
   CurveCounter counter;
   CellSampler<kStorage, kPow2> sampler;
+  StepHistory history{};
 
   while (true) {
     // Hand new particles to idle lanes.
@@ -89,6 +90,7 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
         budget = remaining < a.max_steps ? remaining : a.max_steps;
         it = 0;
         sampler.reset();
+        history.started = false;
         active = true;
         if constexpr (kRecord) {
           // A particle resumed from an earlier launch continues its curve
@@ -121,7 +123,7 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
     if (active) {
       int r = kStepTaken;
       if (it < budget) {
-        r = step<kIntegrator, kStorage, kPow2>(f, a.coefficients, sampler, p);
+        r = step<kIntegrator, kStorage, kPow2>(f, a.coefficients, sampler, p, history);
         if (r == kStepTaken) {
           ++it;
           if constexpr (kRecord) {
@@ -357,6 +359,14 @@ cudaError_t launch_advect(const FieldView& f, const AdvectArgs& a, int integrato
       return launch_storage<DPA_INTEGRATOR_RUNGE_KUTTA_4>(f, a, record, stream);
     case DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE:
       return launch_storage<DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE>(f, a, record, stream);
+    case DPA_INTEGRATOR_MODIFIED_MIDPOINT:
+    case DPA_INTEGRATOR_RUNGE_KUTTA_CASH_KARP_54:
+    case DPA_INTEGRATOR_RUNGE_KUTTA_DORMAND_PRINCE_5:
+    case DPA_INTEGRATOR_RUNGE_KUTTA_FEHLBERG_78:
+    case DPA_INTEGRATOR_ADAMS_BASHFORTH_2:
+    case DPA_INTEGRATOR_ADAMS_BASHFORTH_MOULTON_2:
+      // The coefficients in a.coefficients.g select the stepper.
+      return launch_storage<kGeneralIntegrator>(f, a, record, stream);
     default:
       return cudaErrorInvalidValue;
   }

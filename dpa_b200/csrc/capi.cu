@@ -71,17 +71,13 @@ int check_options(dpa_context* ctx, const dpa_advect_options* o) {
     case DPA_INTEGRATOR_EULER:
     case DPA_INTEGRATOR_RUNGE_KUTTA_4:
     case DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE:
-      break;
     case DPA_INTEGRATOR_MODIFIED_MIDPOINT:
     case DPA_INTEGRATOR_RUNGE_KUTTA_CASH_KARP_54:
     case DPA_INTEGRATOR_RUNGE_KUTTA_DORMAND_PRINCE_5:
     case DPA_INTEGRATOR_RUNGE_KUTTA_FEHLBERG_78:
     case DPA_INTEGRATOR_ADAMS_BASHFORTH_2:
     case DPA_INTEGRATOR_ADAMS_BASHFORTH_MOULTON_2:
-      return fail(ctx, DPA_ERROR_UNSUPPORTED,
-                  "integrator " + std::to_string(o->integrator) +
-                      " is not implemented on the GPU (euler, runge_kutta_4 and "
-                      "runge_kutta_4_true are)");
+      break;
     default:
       return fail(ctx, DPA_ERROR_INVALID_ARGUMENT,
                   "unknown integrator " + std::to_string(o->integrator));
@@ -90,6 +86,10 @@ int check_options(dpa_context* ctx, const dpa_advect_options* o) {
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "step_size is not finite");
   if (o->record && o->max_steps)
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "max_steps applies to calls without recording");
+  if (o->max_steps && dpa::integrator_has_history(o->integrator))
+    return fail(ctx, DPA_ERROR_UNSUPPORTED,
+                "max_steps: this integrator carries a derivative from one step to the next, "
+                "so a particle cannot resume in a later call");
   return DPA_OK;
 }
 
@@ -134,7 +134,7 @@ int advect_device_impl(dpa_context* ctx, const dpa_field* field, const dpa_advec
   a.positions = positions;
   a.remaining = remaining;
   a.termination = termination;
-  a.coefficients = dpa::make_step_coefficients(o->step_size);
+  a.coefficients = dpa::make_step_coefficients(o->integrator, o->step_size);
   DPA_TRY_CUDA(ctx, dpa::launch_advect(field->view, a, o->integrator, false, s));
   ctx->launches += 1;
   if (ctx->profiling) {
@@ -528,7 +528,7 @@ int dpa_advect_round(dpa_context* ctx, const dpa_field* field, const dpa_advect_
   return guarded(ctx, [&]() -> int {
     DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
-    const dpa::StepCoefficients k = dpa::make_step_coefficients(options->step_size);
+    const dpa::StepCoefficients k = dpa::make_step_coefficients(options->integrator, options->step_size);
     if (options->record) {
       for (uint64_t i = 0; i < count; ++i)
         if (remaining[i] > 0xfffffff0ull)
@@ -818,7 +818,7 @@ int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_adve
     DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
     // A sample of the particles, run for at most sample_steps steps each.
-    const uint64_t n = std::min<uint64_t>(count, 1ull << 18);
+    const uint64_t n = std::min<uint64_t>(count, 1ull << 22);
     DeviceBuffer pos, rem, pos0, rem0, term;
     DPA_TRY_CUDA(ctx, pos.reserve(n * 12));
     DPA_TRY_CUDA(ctx, rem.reserve(n * 8));
@@ -828,7 +828,7 @@ int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_adve
     DPA_TRY_CUDA(ctx, cudaMemcpyAsync(pos0.ptr, device_positions, n * 12, cudaMemcpyDeviceToDevice, s));
     DPA_TRY_CUDA(ctx, cudaMemcpyAsync(rem0.ptr, device_remaining, n * 8, cudaMemcpyDeviceToDevice, s));
     dpa_advect_options o = *options;
-    o.max_steps = sample_steps ? sample_steps : 200;
+    if (sample_steps && (o.max_steps == 0 || sample_steps < o.max_steps)) o.max_steps = sample_steps;
     cudaEvent_t e0, e1;
     DPA_TRY_CUDA(ctx, cudaEventCreate(&e0));
     DPA_TRY_CUDA(ctx, cudaEventCreate(&e1));

@@ -6,6 +6,7 @@
 #pragma once
 
 #include <cstdint>
+#include <initializer_list>
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -38,22 +39,125 @@ struct FieldView {
   int32_t pow2;          // every spacing is a power of two (division == product)
 };
 
+// Integrator id of the kernel instantiation shared by the reference's other
+// odeint steppers (modified_midpoint, runge_kutta_cash_karp54,
+// runge_kutta_dopri5, runge_kutta_fehlberg78, adams_bashforth<2>,
+// adams_bashforth_moulton<2>; integrators.hpp:13-28). Their coefficients come
+// with the launch.
+constexpr int kGeneralIntegrator = 1000;
+
+// The reference's system ignores its state argument (particle_advector.cpp:376),
+// so every stage of an odeint step sees the same derivative d and only the
+// stepper's final combination shapes the result. For the general steppers:
+//   kSum:       x_out = 1*x + s[0]*D0 + s[1]*D1 + ... (left to right), where
+//               Di is d, or the particle's previous-step derivative for the
+//               terms in prev_mask once the particle has taken a step;
+//   kMidpoint:  odeint modified_midpoint with 2 sub-steps;
+// and with extrapolated_start a particle's first step is the Adams methods'
+// initialising stepper: extrapolation of modified midpoints with 2 and 4
+// sub-steps.
+enum GeneralKind : int32_t { kGeneralSum = 0, kGeneralMidpoint = 1 };
+
+struct GeneralCoefficients {
+  int32_t kind;
+  int32_t terms;             // entries of s in use (<= 13)
+  uint32_t prev_mask;        // bit i: term i takes the previous step's derivative
+  int32_t extrapolated_start;
+  float s[13];               // b_i * dt (or dt * b_i), each rounded to float
+  float mm2[3];              // 2 sub-steps: h = dt/2, h2 = 2*h, 0.5*h
+  float mm4[3];              // 4 sub-steps: h = dt/4, h2 = 2*h, 0.5*h
+  float ex[2];               // 1 + 1/3 and -(1/3): the single extrapolation
+};
+
 struct StepCoefficients {
   float dt;
   float c0;    // float(1/6) * dt  (odeint rk4 b0 = b3)
   float c1;    // float(1/3) * dt  (odeint rk4 b1 = b2)
   float half;  // float(1/2) * dt  (stage offsets of the four-sample RK4)
+  GeneralCoefficients g;
 };
 
-inline StepCoefficients make_step_coefficients(float dt) {
+// True for the steppers whose step depends on the particle's previous step:
+// runge_kutta_dopri5 (first-same-as-last derivative), adams_bashforth<2>
+// (derivative history) and adams_bashforth_moulton<2> (different first step).
+inline bool integrator_has_history(int integrator) {
+  return integrator == DPA_INTEGRATOR_RUNGE_KUTTA_DORMAND_PRINCE_5 ||
+         integrator == DPA_INTEGRATOR_ADAMS_BASHFORTH_2 ||
+         integrator == DPA_INTEGRATOR_ADAMS_BASHFORTH_MOULTON_2;
+}
+
+// Coefficients as odeint forms them from its float value_type: tableau
+// entries as quotients of floats, then products with dt in float.
+inline StepCoefficients make_step_coefficients(int integrator, float dt) {
   volatile float b0 = 1.0f / 6.0f;  // computed in float as odeint does
   volatile float b1 = 1.0f / 3.0f;
   volatile float a = 1.0f / 2.0f;
-  StepCoefficients k;
+  StepCoefficients k{};
   k.dt = dt;
   k.c0 = b0 * dt;
   k.c1 = b1 * dt;
   k.half = a * dt;
+  GeneralCoefficients& g = k.g;
+  auto q = [](float num, float den) {
+    volatile float n = num, d = den;
+    return n / d;
+  };
+  auto sum = [&](std::initializer_list<float> b, bool dt_first) {
+    g.kind = kGeneralSum;
+    g.terms = 0;
+    for (float v : b) {
+      volatile float bv = v, t = dt;
+      g.s[g.terms++] = dt_first ? t * bv : bv * t;
+    }
+  };
+  for (int m = 0; m < 2; ++m) {
+    float* mm = m == 0 ? g.mm2 : g.mm4;
+    volatile float steps = m == 0 ? 2.0f : 4.0f;
+    const float h = dt / steps;
+    mm[0] = h;
+    mm[1] = 2.0f * h;
+    mm[2] = 0.5f * h;
+  }
+  {
+    volatile float four = 4.0f, two = 2.0f, one = 1.0f;
+    const float r = four / two;
+    const float c = one / (r * r - one);
+    g.ex[0] = one + c;
+    g.ex[1] = -c;
+  }
+  switch (integrator) {
+    case DPA_INTEGRATOR_MODIFIED_MIDPOINT:
+      g.kind = kGeneralMidpoint;
+      break;
+    case DPA_INTEGRATOR_RUNGE_KUTTA_CASH_KARP_54:
+      // rk54_ck: 5th-order weights (do_step without error estimate).
+      sum({q(37, 378), 0.0f, q(250, 621), q(125, 594), 0.0f, q(512, 1771)}, false);
+      break;
+    case DPA_INTEGRATOR_RUNGE_KUTTA_DORMAND_PRINCE_5:
+      // dopri5: x + dt*c1*dxdt_in + dt*c3*k3 + dt*c4*k4 + dt*c5*k5 + dt*c6*k6;
+      // dxdt_in is the derivative the previous step left behind.
+      sum({q(35, 384), q(500, 1113), q(125, 192), q(-2187, 6784), q(11, 84)}, true);
+      g.prev_mask = 1u;
+      break;
+    case DPA_INTEGRATOR_RUNGE_KUTTA_FEHLBERG_78:
+      sum({0.0f, 0.0f, 0.0f, 0.0f, 0.0f, q(34, 105), q(9, 35), q(9, 35), q(9, 280), q(9, 280),
+           0.0f, q(41, 840), q(41, 840)},
+          false);
+      break;
+    case DPA_INTEGRATOR_ADAMS_BASHFORTH_2:
+      // x + dt*(3/2)*d_n + dt*(-1/2)*d_(n-1)
+      sum({q(3, 2), -q(1, 2)}, true);
+      g.prev_mask = 2u;
+      g.extrapolated_start = 1;
+      break;
+    case DPA_INTEGRATOR_ADAMS_BASHFORTH_MOULTON_2:
+      // Corrector x + dt*(1/2)*f(predicted) + dt*(1/2)*d_n, both equal to d_n.
+      sum({q(1, 2), q(1, 2)}, true);
+      g.extrapolated_start = 1;
+      break;
+    default:
+      break;
+  }
   return k;
 }
 

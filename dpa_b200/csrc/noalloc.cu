@@ -80,12 +80,14 @@ extern "C" int dpa_advect_device_no_alloc(dpa_context* ctx, const dpa_field* fie
     if (options->record)
       return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT,
                     "dpa_advect_device_no_alloc does not record; use dpa_advect_round");
-    if (options->integrator != DPA_INTEGRATOR_EULER &&
-        options->integrator != DPA_INTEGRATOR_RUNGE_KUTTA_4 &&
-        options->integrator != DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE)
+    if (!((options->integrator >= DPA_INTEGRATOR_EULER &&
+           options->integrator <= DPA_INTEGRATOR_ADAMS_BASHFORTH_MOULTON_2) ||
+          options->integrator == DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE))
+      return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT, "unknown integrator");
+    if (options->max_steps && dpa::integrator_has_history(options->integrator))
       return refuse(ctx, DPA_ERROR_UNSUPPORTED,
-                    "integrator not implemented on the GPU (euler, runge_kutta_4 and "
-                    "runge_kutta_4_true are)");
+                    "max_steps: this integrator carries a derivative from one step to the "
+                    "next, so a particle cannot resume in a later call");
     if (count > kMaxParticles)
       return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT,
                     "dpa_advect_device_no_alloc: count exceeds DPA_NO_ALLOC_MAX_PARTICLES "
@@ -122,7 +124,7 @@ extern "C" int dpa_advect_device_no_alloc(dpa_context* ctx, const dpa_field* fie
     a.positions = device_positions;
     a.remaining = device_remaining;
     a.termination = device_termination;
-    a.coefficients = dpa::make_step_coefficients(options->step_size);
+    a.coefficients = dpa::make_step_coefficients(options->integrator, options->step_size);
     e = dpa::launch_advect(field->view, a, options->integrator, false, s);
     if (e != cudaSuccess) return refuse_cuda(ctx, e, "advection kernel");
     return DPA_OK;

@@ -210,11 +210,79 @@ __device__ __forceinline__ bool is_zero(float2 v01, float v2) {
 
 enum StepResult : int { kStepTaken = 0, kStepOutOfBounds = 1, kStepZeroVelocity = 2 };
 
+// What the general steppers keep of a particle's previous step: its
+// derivative (as v01, v2) and whether the particle has taken a step yet.
+// Every particle starts fresh, as the reference copies its integrator per
+// particle (particle_advector.cpp:335).
+struct StepHistory {
+  float2 d01;
+  float d2;
+  bool started;
+};
+
+// odeint modified_midpoint with kSteps sub-steps and the state-independent
+// derivative d, one component: m_x1 = x + h d; kSteps - 1 times
+// (m_x1, m_x0) = (m_x0 + h2 d, m_x1); out = 0.5 m_x0 + 0.5 m_x1 + (0.5 h) d.
+// mm = {h, h2, 0.5 h}.
+template <int kSteps>
+__device__ __forceinline__ float modified_midpoint(float x, float d, const float* mm) {
+  float x1 = __fadd_rn(x, __fmul_rn(mm[0], d));
+  float x0 = x;
+#pragma unroll
+  for (int i = 1; i < kSteps; ++i) {
+    const float t = x1;
+    x1 = __fadd_rn(x0, __fmul_rn(mm[1], d));
+    x0 = t;
+  }
+  return __fadd_rn(__fadd_rn(__fmul_rn(0.5f, x0), __fmul_rn(0.5f, x1)), __fmul_rn(mm[2], d));
+}
+
+// The Adams methods' initialising stepper (an order-4 extrapolation
+// stepper): modified midpoints with 2 and 4 sub-steps, one polynomial
+// extrapolation x = (1 + c) mm4 + (-c) mm2, c = 1/3.
+__device__ __forceinline__ float extrapolated_start(float x, float d, const GeneralCoefficients& g) {
+  const float a = modified_midpoint<2>(x, d, g.mm2);
+  const float b = modified_midpoint<4>(x, d, g.mm4);
+  return __fadd_rn(__fmul_rn(g.ex[0], b), __fmul_rn(g.ex[1], a));
+}
+
+// One step of a general stepper (kGeneralIntegrator) given this step's
+// derivative; updates the history.
+__device__ __forceinline__ void general_step(const GeneralCoefficients& g, float2 v01, float v2,
+                                             StepHistory& h, Position& p) {
+  if (g.kind == kGeneralMidpoint) {
+    p.p0 = modified_midpoint<2>(p.p0, v2, g.mm2);
+    p.p21 = make_float2(modified_midpoint<2>(p.p21.x, v01.x, g.mm2),
+                        modified_midpoint<2>(p.p21.y, v01.y, g.mm2));
+  } else if (g.extrapolated_start && !h.started) {
+    p.p0 = extrapolated_start(p.p0, v2, g);
+    p.p21 = make_float2(extrapolated_start(p.p21.x, v01.x, g),
+                        extrapolated_start(p.p21.y, v01.y, g));
+  } else {
+    float x0 = p.p0, xa = p.p21.x, xb = p.p21.y;
+#pragma unroll
+    for (int i = 0; i < 13; ++i) {
+      if (i < g.terms) {
+        const bool prev = h.started && ((g.prev_mask >> i) & 1u);
+        x0 = __fadd_rn(x0, __fmul_rn(g.s[i], prev ? h.d2 : v2));
+        xa = __fadd_rn(xa, __fmul_rn(g.s[i], prev ? h.d01.x : v01.x));
+        xb = __fadd_rn(xb, __fmul_rn(g.s[i], prev ? h.d01.y : v01.y));
+      }
+    }
+    p.p0 = x0;
+    p.p21 = make_float2(xa, xb);
+  }
+  h.d01 = v01;
+  h.d2 = v2;
+  h.started = true;
+}
+
 // One integrator step in place. The derivative of p0 is v2 and that of
 // (p2, p1) is (v0, v1) (particle_advector.cpp:369).
 template <int kIntegrator, int kStorage, bool kPow2>
 __device__ __forceinline__ int step(const FieldView& f, const StepCoefficients& k,
-                                   CellSampler<kStorage, kPow2>& sampler, Position& p) {
+                                   CellSampler<kStorage, kPow2>& sampler, Position& p,
+                                   StepHistory& history) {
   float2 v01;
   float v2;
   if (!sampler.sample(f, p, v01, v2)) return kStepOutOfBounds;
@@ -230,6 +298,8 @@ __device__ __forceinline__ int step(const FieldView& f, const StepCoefficients& 
     p.p0 = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(p.p0, m0), m1), m1), m0);
     const float2 n0 = mul2(splat(k.c0), v01), n1 = mul2(splat(k.c1), v01);
     p.p21 = add2(add2(add2(add2(p.p21, n0), n1), n1), n0);
+  } else if constexpr (kIntegrator == kGeneralIntegrator) {
+    general_step(k.g, v01, v2, history, p);
   } else {
     // Four-sample RK4; a stage outside the grid ends the particle without
     // taking the step.

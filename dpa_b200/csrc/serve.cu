@@ -157,9 +157,13 @@ namespace {
       throw std::runtime_error(std::string(#expr) + ": " + cudaGetErrorName(e_)); \
   } while (0)
 
+// Requests advance in step budgets of steps_per_tick, so a particle resumes
+// in a later tick: integrators that carry a derivative from one step to the
+// next (dpa::integrator_has_history) are not served.
 bool integrator_ok(int32_t i) {
-  return i == DPA_INTEGRATOR_EULER || i == DPA_INTEGRATOR_RUNGE_KUTTA_4 ||
-         i == DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE;
+  const bool known = (i >= DPA_INTEGRATOR_EULER && i <= DPA_INTEGRATOR_ADAMS_BASHFORTH_MOULTON_2) ||
+                     i == DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE;
+  return known && !dpa::integrator_has_history(i);
 }
 
 }  // namespace
@@ -263,7 +267,7 @@ bool dpa_server::tick() {
     a.positions = positions.as<float>();
     a.remaining = remaining.as<uint64_t>();
     a.termination = termination.as<uint8_t>();
-    a.coefficients = dpa::make_step_coefficients(step_size);
+    a.coefficients = dpa::make_step_coefficients(integrator, step_size);
     a.max_steps = options.steps_per_tick ? options.steps_per_tick : 64;
     a.claim = ctx->tuning.claim;
     a.work_counter = work_counter.as<unsigned long long>();

@@ -50,12 +50,16 @@ typedef enum dpa_storage {
 
 /* Integrators. Codes 0-7 follow the alternatives of the reference's
  * variant_integrator (include/dpa/types/integrators.hpp:31-39) and the names
- * of particle_advector.cpp:29-36. The GPU implements euler and
- * runge_kutta_4; the others return DPA_ERROR_UNSUPPORTED.
- * DPA_INTEGRATOR_RUNGE_KUTTA_4 has the reference's semantics: its system
- * functor (particle_advector.cpp:369) samples the field once per step, so all
- * four stages see the same derivative. DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE
- * samples at all four stages (no counterpart in the reference). */
+ * of particle_advector.cpp:29-36, with the reference's semantics: its system
+ * functor (particle_advector.cpp:376) samples the field once per step, so
+ * every stage of a step sees the same derivative and each odeint stepper
+ * reduces to its final combination. runge_kutta_dormand_prince_5 (its
+ * first-same-as-last derivative is the previous step's sample),
+ * adams_bashforth_2 (derivative history) and adams_bashforth_moulton_2
+ * (extrapolated first step) depend on a particle's earlier steps: calls with
+ * max_steps and the request server refuse them (DPA_ERROR_UNSUPPORTED).
+ * DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE samples at all four stages (no
+ * counterpart in the reference). */
 typedef enum dpa_integrator {
   DPA_INTEGRATOR_EULER = 0,
   DPA_INTEGRATOR_MODIFIED_MIDPOINT = 1,
@@ -237,9 +241,12 @@ int dpa_context_set_tuning(dpa_context* ctx, const dpa_tuning* tuning);
 int dpa_context_get_tuning(const dpa_context* ctx, dpa_tuning* tuning);
 
 /* Times the candidate settings (claim 16..128, 2 to all resident blocks per SM,
- * order 16 / 8 / off) on a sample of up to 262,144 of the given device
- * particles, each advanced at most sample_steps steps (0: 200) on copies,
- * keeps the fastest in the context and returns it in best (may be NULL). */
+ * order 16 / 8 / off) on copies of the first min(count, 4,194,304) of the
+ * given device particles, each advanced at most sample_steps steps (0: its
+ * whole remaining budget, capped by options->max_steps), keeps the fastest in
+ * the context and returns it in best (may be NULL). The processing order pays
+ * off with particle density and run length, so a sample as dense and as long
+ * as the real run picks the setting that run wants. */
 int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_advect_options* options,
                         uint64_t count, const float* device_positions,
                         const uint64_t* device_remaining, uint64_t sample_steps,

@@ -14,7 +14,11 @@ ORACLE_DIR = Path(__file__).resolve().parent
 ORACLE_LIB = ORACLE_DIR / "liboracle.so"
 
 EULER, RK4, RK4_TRUE = 0, 2, 100
-INTEGRATOR_CODES = {"euler": EULER, "runge_kutta_4": RK4, "runge_kutta_4_true": RK4_TRUE}
+# include/dpa/types/integrators.hpp:31-39 order; 100 has no reference counterpart.
+INTEGRATOR_CODES = {"euler": EULER, "modified_midpoint": 1, "runge_kutta_4": RK4,
+                    "runge_kutta_cash_karp_54": 3, "runge_kutta_dormand_prince_5": 4,
+                    "runge_kutta_fehlberg_78": 5, "adams_bashforth_2": 6,
+                    "adams_bashforth_moulton_2": 7, "runge_kutta_4_true": RK4_TRUE}
 
 
 class Grid(C.Structure):

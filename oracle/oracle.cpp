@@ -13,7 +13,13 @@
 //     vector_space_algebra. The final stage is one scale_sum5 expression
 //     x_out = 1*x + (b0*dt)*k1 + (b1*dt)*k2 + (b2*dt)*k3 + (b3*dt)*k4,
 //     evaluated left to right per component, with b = {1/6, 1/3, 1/3, 1/6}
-//     computed in float.
+//     computed in float. The other steppers of integrators.hpp:13-28 follow
+//     odeint's published algorithms as of Boost 1.6x-1.8x (odeint_step
+//     below): modified_midpoint with its default 2 sub-steps, the
+//     runge_kutta_cash_karp54 / runge_kutta_fehlberg78 high-order weights,
+//     runge_kutta_dopri5 with its first-same-as-last derivative, and
+//     adams_bashforth<2> / adams_bashforth_moulton<2>, whose first step is
+//     their default initialising stepper, extrapolation_stepper<4>.
 //   * Eigen >= 3.3 (version not pinned): isZero() with the float dummy
 //     precision 1e-5; fixed-size 3-element reductions (squaredNorm, dot,
 //     lazy 3x3 product coefficients) unrolled as c0 + (c1 + c2);
@@ -158,6 +164,121 @@ step_coefficients make_coefficients(float dt) {
 }
 
 // ---------------------------------------------------------------------------
+// The other odeint steppers (integrators.hpp:13-28) as the reference calls
+// them: integrator.do_step(system, position, t, dt) once per iteration with a
+// system that ignores its state and time arguments and returns this
+// iteration's sample d (particle_advector.cpp:376-393). Every stage
+// derivative inside one do_step is therefore d, and the stage states odeint
+// forms are never read; what remains is each stepper's final expression,
+// evaluated per component left to right in float. Tableau entries are
+// quotients of floats (odeint's static_cast<value_type>(p) / q).
+// ---------------------------------------------------------------------------
+inline float fq(float p, float q) { return p / q; }
+
+struct odeint_state {
+  bool  started = false;  // the per-particle integrator copy has stepped
+  float fsal[3] = {0, 0, 0};   // dopri5: derivative left by the last step
+  float history[3] = {0, 0, 0};  // adams_bashforth: d of the previous step
+};
+
+// modified_midpoint::do_step_impl with `steps` sub-steps and constant d:
+// h = dt / steps, h2 = 2 h; x1 = 1*x + h*d; x0 = x; (steps - 1) times
+// scale_sum_swap2: (x1, x0) = (1*x0 + h2*d, x1); out = 0.5*x0 + 0.5*x1 + (0.5*h)*d.
+float odeint_modified_midpoint(float x, float d, float dt, unsigned steps) {
+  const float h = dt / static_cast<float>(steps);
+  const float h2 = 2.0f * h;
+  float x1 = 1.0f * x + h * d;
+  float x0 = x;
+  for (unsigned i = 1; i != steps; ++i) {
+    const float tmp = x1;
+    x1 = 1.0f * x0 + h2 * d;
+    x0 = tmp;
+  }
+  return 0.5f * x0 + 0.5f * x1 + (0.5f * h) * d;
+}
+
+// extrapolation_stepper<4>::do_step_impl: interval sequence {2, 4}; out =
+// midpoint(2); table[0] = midpoint(4); extrapolate(k = 1):
+// out = (1 + c) * table[0] + (-c) * out with c = 1 / ((4/2)^2 - 1).
+float odeint_extrapolation4(float x, float d, float dt) {
+  const float r = static_cast<float>(4) / static_cast<float>(2);
+  const float c = static_cast<float>(1) / (r * r - static_cast<float>(1));
+  const float m2 = odeint_modified_midpoint(x, d, dt, 2);
+  const float m4 = odeint_modified_midpoint(x, d, dt, 4);
+  return (static_cast<float>(1) + c) * m4 + (-c) * m2;
+}
+
+void odeint_step(int integrator, float dt, const float* d, odeint_state& st, float* x) {
+  switch (integrator) {
+    case ORACLE_MODIFIED_MIDPOINT:
+      for (int c = 0; c < 3; ++c) x[c] = odeint_modified_midpoint(x[c], d[c], dt, 2);
+      break;
+    case ORACLE_RUNGE_KUTTA_CASH_KARP_54: {
+      // explicit_error_generic_rk<6,5,5,4>::do_step without error: final
+      // scale_sum7(1, b0*dt, ..., b5*dt) with the 5th-order weights.
+      const float b[6] = {fq(37, 378), 0.0f, fq(250, 621), fq(125, 594), 0.0f, fq(512, 1771)};
+      for (int c = 0; c < 3; ++c) {
+        float v = 1.0f * x[c];
+        for (int i = 0; i < 6; ++i) v = v + (b[i] * dt) * d[c];
+        x[c] = v;
+      }
+      break;
+    }
+    case ORACLE_RUNGE_KUTTA_DORMAND_PRINCE_5: {
+      // explicit_error_stepper_fsal_base::do_step: on the first call
+      // initialize() evaluates dxdt = system(x); afterwards dxdt is the
+      // derivative the previous do_step_impl ended with (system(out), i.e.
+      // that step's sample). x_out = 1*x + dt*c1*dxdt + dt*c3*k3 + dt*c4*k4 +
+      // dt*c5*k5 + dt*c6*k6, then the new dxdt = system(x_out) = d.
+      const float c1 = fq(35, 384), c3 = fq(500, 1113), c4 = fq(125, 192),
+                  c5 = fq(-2187, 6784), c6 = fq(11, 84);
+      if (!st.started) std::memcpy(st.fsal, d, sizeof st.fsal);
+      for (int c = 0; c < 3; ++c)
+        x[c] = 1.0f * x[c] + (dt * c1) * st.fsal[c] + (dt * c3) * d[c] + (dt * c4) * d[c] +
+               (dt * c5) * d[c] + (dt * c6) * d[c];
+      std::memcpy(st.fsal, d, sizeof st.fsal);
+      break;
+    }
+    case ORACLE_RUNGE_KUTTA_FEHLBERG_78: {
+      // explicit_error_generic_rk<13,8,8,7>: final scale_sum14 with the
+      // 8th-order weights.
+      const float b[13] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, fq(34, 105), fq(9, 35), fq(9, 35),
+                           fq(9, 280), fq(9, 280), 0.0f, fq(41, 840), fq(41, 840)};
+      for (int c = 0; c < 3; ++c) {
+        float v = 1.0f * x[c];
+        for (int i = 0; i < 13; ++i) v = v + (b[i] * dt) * d[c];
+        x[c] = v;
+      }
+      break;
+    }
+    case ORACLE_ADAMS_BASHFORTH_2:
+    case ORACLE_ADAMS_BASHFORTH_MOULTON_2: {
+      if (!st.started) {
+        // adams_bashforth::do_step_impl before 1 step is stored: the
+        // initialising stepper advances, the step storage keeps d.
+        for (int c = 0; c < 3; ++c) x[c] = odeint_extrapolation4(x[c], d[c], dt);
+      } else if (integrator == ORACLE_ADAMS_BASHFORTH_2) {
+        // rotate, store d; scale_sum3(1, dt*(3/2), dt*(-1/2)) of (x, d_n, d_n-1).
+        const float a0 = fq(3, 2), a1 = -fq(1, 2);
+        for (int c = 0; c < 3; ++c)
+          x[c] = 1.0f * x[c] + (dt * a0) * d[c] + (dt * a1) * st.history[c];
+      } else {
+        // adams_bashforth_moulton: the AB2 predictor only feeds the system,
+        // which ignores it; the AM2 corrector is scale_sum3(1, dt*(1/2),
+        // dt*(1/2)) of (x, system(predicted), d_n).
+        const float m0 = fq(1, 2), m1 = fq(1, 2);
+        for (int c = 0; c < 3; ++c) x[c] = 1.0f * x[c] + (dt * m0) * d[c] + (dt * m1) * d[c];
+      }
+      std::memcpy(st.history, d, sizeof st.history);
+      break;
+    }
+    default:
+      break;
+  }
+  st.started = true;
+}
+
+// ---------------------------------------------------------------------------
 // particle_advector::advect, one particle (particle_advector.cpp:325-396)
 // ---------------------------------------------------------------------------
 std::uint8_t advect_one(const oracle_grid& g, int integrator, const step_coefficients& k,
@@ -165,6 +286,7 @@ std::uint8_t advect_one(const oracle_grid& g, int integrator, const step_coeffic
                         float* curve /* null or curve_stride * 3 floats */) {
   std::uint64_t iteration = 0;
   std::uint8_t reason = ORACLE_COMPLETE;
+  odeint_state state;  // `auto integrator = integrator_;` per particle (:335)
   if (curve) std::memcpy(curve, pos, 3 * sizeof(float));
   for (; *remaining > 0; ++iteration, --*remaining) {
     if (!grid_contains(g, pos)) { reason = ORACLE_OUT_OF_BOUNDS; break; }
@@ -181,6 +303,8 @@ std::uint8_t advect_one(const oracle_grid& g, int integrator, const step_coeffic
       // derivative equals d, so only the final scale_sum5 remains.
       for (int c = 0; c < 3; ++c)
         pos[c] = 1.0f * pos[c] + k.c0 * d[c] + k.c1 * d[c] + k.c1 * d[c] + k.c0 * d[c];
+    } else if (integrator != ORACLE_RUNGE_KUTTA_4_TRUE) {
+      odeint_step(integrator, k.dt, d, state, pos);
     } else {
       // Four-sample RK4 (not part of the reference): stages at x,
       // x + dt/2 k1, x + dt/2 k2, x + dt k3; a stage outside the grid ends
@@ -343,8 +467,8 @@ int oracle_advect_round(const oracle_grid* grid, int integrator, float step_size
                         uint8_t* termination, uint64_t* steps,
                         int record, uint64_t curve_stride, float* raw_vertices) {
   if (!grid || (count && (!positions || !remaining))) return 1;
-  if (integrator != ORACLE_EULER && integrator != ORACLE_RUNGE_KUTTA_4 &&
-      integrator != ORACLE_RUNGE_KUTTA_4_TRUE)
+  if (!((integrator >= ORACLE_EULER && integrator <= ORACLE_ADAMS_BASHFORTH_MOULTON_2) ||
+        integrator == ORACLE_RUNGE_KUTTA_4_TRUE))
     return 2;
   if (record) {
     if (!raw_vertices) return 1;
@@ -543,6 +667,9 @@ int oracle64_advect(const oracle_grid* grid, int integrator, double step_size,
                     uint64_t count, double* positions, uint64_t* remaining,
                     uint8_t* termination, uint64_t* steps) {
   if (!grid) return 1;
+  if (integrator != ORACLE_EULER && integrator != ORACLE_RUNGE_KUTTA_4 &&
+      integrator != ORACLE_RUNGE_KUTTA_4_TRUE)
+    return 2;
   const oracle_grid& g = *grid;
   const int threads = oracle_get_threads();
 #pragma omp parallel for schedule(dynamic, 64) num_threads(threads)

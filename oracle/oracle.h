@@ -38,11 +38,18 @@ typedef struct oracle_grid {
 } oracle_grid;
 
 /* Integrator codes follow the order of the reference's integrator variant
- * (include/dpa/types/integrators.hpp:31-39). Only euler and runge_kutta_4 are
- * restated; 100 is the four-sample Runge-Kutta 4 used by the FP64 oracle. */
+ * (include/dpa/types/integrators.hpp:31-39); 100 is the four-sample
+ * Runge-Kutta 4 (no counterpart in the reference). The FP64 oracle takes
+ * euler, runge_kutta_4 and 100 only. */
 enum {
   ORACLE_EULER = 0,
+  ORACLE_MODIFIED_MIDPOINT = 1,
   ORACLE_RUNGE_KUTTA_4 = 2,
+  ORACLE_RUNGE_KUTTA_CASH_KARP_54 = 3,
+  ORACLE_RUNGE_KUTTA_DORMAND_PRINCE_5 = 4,
+  ORACLE_RUNGE_KUTTA_FEHLBERG_78 = 5,
+  ORACLE_ADAMS_BASHFORTH_2 = 6,
+  ORACLE_ADAMS_BASHFORTH_MOULTON_2 = 7,
   ORACLE_RUNGE_KUTTA_4_TRUE = 100
 };
 

@@ -150,13 +150,43 @@ def test_edge_cases(ctx, oracle):
     assert list(out.inactive_particles.remaining_iterations) == [9, 9, 9]
 
 
-def test_unsupported_integrators_report_an_error(ctx):
+OTHER_INTEGRATORS = ["modified_midpoint", "runge_kutta_cash_karp_54",
+                     "runge_kutta_dormand_prince_5", "runge_kutta_fehlberg_78",
+                     "adams_bashforth_2", "adams_bashforth_moulton_2"]
+
+
+@pytest.mark.parametrize("integrator", OTHER_INTEGRATORS)
+def test_other_odeint_steppers_match_oracle(ctx, oracle, integrator):
+    # Recorded curves over several rounds, then end positions on a
+    # power-of-two grid with FP16 storage (the multiplicative cell lookup).
+    grid = fields.abc(48)
+    pos = _seeds_in_box(grid, 700, 3, ([0, 0, 0], [2 * math.pi] * 3))
+    compare(ctx, oracle, grid, pos, 200, integrator, 0.02, 256, True)
+    noise = fields.curl_noise(64, 4.0, 6)
+    pos = _seeds_in_box(noise, 3000, 4)
+    compare(ctx, oracle, noise, pos, 400, integrator, 0.25, 3000, False, storage="f16")
+
+
+@pytest.mark.parametrize("integrator", ["runge_kutta_dormand_prince_5", "adams_bashforth_2",
+                                        "adams_bashforth_moulton_2"])
+def test_steppers_with_memory_refuse_step_budgets(ctx, integrator):
+    import ctypes as C
+    import torch
+    from dpa_b200 import _native as N
     grid = fields.abc(8)
     field = ctx.field(grid)
-    adv = ParticleAdvector(ctx, 4, "none", "runge_kutta_dormand_prince_5", 0.1, False, False)
-    with pytest.raises(dpa_b200.DpaError) as e:
-        adv.advect(field, Particles.create(np.ones((2, 3), np.float32), 3))
-    assert e.value.status == 2
+    pos = torch.ones((2, 3), dtype=torch.float32, device="cuda")
+    rem = torch.full((2,), 3, dtype=torch.int64, device="cuda")
+    opts = N.AdvectOptions(N.INTEGRATORS[integrator], 0.1, 0, 0, 0, 0, 2)
+    rc = ctx._lib.dpa_advect_device(ctx.handle, field.handle, C.byref(opts), 2,
+                                    C.c_void_p(pos.data_ptr()), C.c_void_p(rem.data_ptr()), None,
+                                    None)
+    assert rc == 2
+    rc = ctx._lib.dpa_advect_device_no_alloc(ctx.handle, field.handle, C.byref(opts), 2,
+                                             C.c_void_p(pos.data_ptr()),
+                                             C.c_void_p(rem.data_ptr()), None, None)
+    assert rc == 2
+    field.close()
 
 
 def test_device_api_matches_host_api(ctx, oracle):

@@ -158,3 +158,23 @@ def test_many_concurrent_requests_all_complete(ctx, resident):
         np.testing.assert_array_equal(got[rid].termination, want.inactive_particles.termination)
         assert got[rid].particle_steps == int(
             (iters - want.inactive_particles.remaining_iterations.astype(np.int64)).sum())
+
+
+def test_server_takes_memoryless_steppers_and_refuses_the_others(ctx, resident):
+    grid, field = resident["abc"]
+    offset, size = seeds.seed_box(grid)
+    pos = seeds.generate_random(offset, size, 500, 80, seed=8).position
+    with Server(ctx, particle_capacity=5000, vertex_capacity=1_000_000, steps_per_tick=16,
+                max_requests=4) as server:
+        fid = server.add_field(field)
+        for name in ("runge_kutta_dormand_prince_5", "adams_bashforth_2",
+                     "adams_bashforth_moulton_2"):
+            with pytest.raises(dpa_b200.DpaError) as e:
+                server.submit(fid, pos, 80, name, 0.02)
+            assert e.value.status == 2
+        server.submit(fid, pos, 80, "runge_kutta_cash_karp_54", 0.02, record=True)
+        res = server.poll(wait_ms=5000)
+    assert res is not None and res.status == 0
+    want = alone(ctx, field, pos, 80, "runge_kutta_cash_karp_54", 0.02, True)
+    np.testing.assert_array_equal(res.positions, want.inactive_particles.position)
+    np.testing.assert_array_equal(res.vertices, want.integral_curves[0].vertices)
