@@ -14,10 +14,11 @@ is the host-side mirror of the reference's stage interface over that ABI:
 """
 from ._native import DpaError, load as load_library
 from .advector import (AdvectOutput, Context, Field, IntegralCurve, ParticleAdvector, Particles,
-                       RegularGrid, estimate_ftle)
+                       PathlineResult, RegularGrid, UnsteadyGrid, advect_pathlines, estimate_ftle)
 from . import fields, seeds
 
 __all__ = [
     "AdvectOutput", "Context", "DpaError", "Field", "IntegralCurve", "ParticleAdvector",
-    "Particles", "RegularGrid", "estimate_ftle", "fields", "load_library", "seeds",
+    "Particles", "PathlineResult", "RegularGrid", "UnsteadyGrid", "advect_pathlines",
+    "estimate_ftle", "fields", "load_library", "seeds",
 ]

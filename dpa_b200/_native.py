@@ -99,6 +99,7 @@ class Request(C.Structure):
         ("positions", C.POINTER(C.c_float)),
         ("iterations", C.c_uint64),
         ("user", C.c_void_p),
+        ("start_time", C.c_float),
     ]
 
 
@@ -122,6 +123,7 @@ class Response(C.Structure):
         ("queued_seconds", C.c_double),
         ("admitted_seconds", C.c_double),
         ("finished_seconds", C.c_double),
+        ("times", C.POINTER(C.c_float)),
     ]
 
 
@@ -164,9 +166,14 @@ SIGNATURES = {
                                           C.POINTER(C.c_void_p)]),
     "dpa_field_destroy": (C.c_int, [_P, _P]),
     "dpa_field_info": (C.c_int, [_P, _U64P, _F32P, _F32P, C.POINTER(C.c_int32), _U64P]),
+    "dpa_field_create_unsteady": (C.c_int, [_P, _P, _U64P, C.c_uint32, _F32P, _F32P, C.c_float,
+                                            C.c_float, C.c_int32, C.POINTER(C.c_void_p)]),
+    "dpa_field_time_info": (C.c_int, [_P, C.POINTER(C.c_uint32), _F32P, _F32P]),
     "dpa_advect_round": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _P, _P, _P,
                                    CURVE_SINK, _P]),
     "dpa_advect_device": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _P, _P, _P, _P]),
+    "dpa_advect_pathlines_device": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _P, _P,
+                                              _P, _P, _P]),
     "dpa_advect_batch_device": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _U64P,
                                           _P, _P, _P, _U64P, _P]),
     "dpa_graph_create_advect": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _P, _P,

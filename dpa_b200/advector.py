@@ -43,6 +43,40 @@ class RegularGrid:
 
 
 @dataclass
+class UnsteadyGrid:
+    """A time-varying field (no counterpart in the reference): `slices` grids
+    of one shape, data [slices][n0][n1][n2][3], slice s at time
+    time_origin + s * time_spacing."""
+
+    data: np.ndarray
+    offset: np.ndarray
+    spacing: np.ndarray
+    time_origin: float
+    time_spacing: float
+
+    @staticmethod
+    def from_data(data: np.ndarray, spacing, time_spacing: float, offset=(0.0, 0.0, 0.0),
+                  time_origin: float = 0.0) -> "UnsteadyGrid":
+        data = np.ascontiguousarray(data, dtype=np.float32)
+        if data.ndim != 5 or data.shape[-1] != 3 or data.shape[0] < 2:
+            raise ValueError("expected data of shape [slices >= 2][n0][n1][n2][3]")
+        return UnsteadyGrid(data, np.asarray(offset, np.float32).reshape(3),
+                            np.asarray(spacing, np.float32).reshape(3),
+                            float(np.float32(time_origin)), float(np.float32(time_spacing)))
+
+    @property
+    def shape(self) -> tuple[int, int, int]:
+        return tuple(int(s) for s in self.data.shape[1:4])
+
+    @property
+    def slices(self) -> int:
+        return int(self.data.shape[0])
+
+    def slice(self, s: int) -> RegularGrid:
+        return RegularGrid.from_data(self.data[s], self.spacing, self.offset)
+
+
+@dataclass
 class Particles:
     """Structure-of-arrays form of particle_3d (include/dpa/types/particle.hpp:12-77)."""
 
@@ -148,7 +182,16 @@ class Field:
         self.storage = storage
         handle = C.c_void_p()
         lib = context._lib
-        if device_pointer is None:
+        if isinstance(grid, UnsteadyGrid):
+            if device_pointer is not None:
+                raise ValueError("time-varying fields are uploaded from host memory")
+            data = np.ascontiguousarray(grid.data, dtype=np.float32)
+            st = lib.dpa_field_create_unsteady(context.handle, data.ctypes.data_as(C.c_void_p),
+                                               _u3(grid.shape), grid.slices, _f3(grid.offset),
+                                               _f3(grid.spacing), grid.time_origin,
+                                               grid.time_spacing, N.STORAGE[storage],
+                                               C.byref(handle))
+        elif device_pointer is None:
             data = np.ascontiguousarray(grid.data, dtype=np.float32)
             st = lib.dpa_field_create(context.handle, data.ctypes.data_as(C.c_void_p),
                                       _u3(grid.shape), _f3(grid.offset), _f3(grid.spacing),
@@ -323,3 +366,35 @@ def estimate_ftle(context: Context, field: Field, seed_maximum_iterations: int, 
                                         out.ctypes.data_as(C.c_void_p), shape))
     spacing = (field.grid.spacing * np.asarray(seed_stride, dtype=np.float32)).astype(np.float32)
     return RegularGrid(out, field.grid.offset.copy(), field.grid.size.copy(), spacing)
+
+
+@dataclass
+class PathlineResult:
+    position: np.ndarray
+    time: np.ndarray
+    remaining_iterations: np.ndarray
+    termination: np.ndarray
+
+
+def advect_pathlines(context: Context, field: Field, positions, times, iterations,
+                     integrator: str = "runge_kutta_4", step_size: float = 0.25,
+                     max_steps: int = 0, morton_order: bool = True) -> PathlineResult:
+    """Pathlines (end states) through a field, each particle starting at its
+    own time, via dpa_advect_pathlines_device on device copies of the inputs."""
+    import torch
+    pos = torch.from_numpy(np.ascontiguousarray(positions, np.float32).reshape(-1, 3)).cuda()
+    n = pos.shape[0]
+    t = torch.from_numpy(np.broadcast_to(np.asarray(times, np.float32), (n,)).copy()).cuda()
+    rem = torch.from_numpy(
+        np.broadcast_to(np.asarray(iterations, np.uint64), (n,)).astype(np.int64)).cuda()
+    term = torch.zeros(n, dtype=torch.uint8, device="cuda")
+    opts = N.AdvectOptions(N.INTEGRATORS[integrator], float(np.float32(step_size)), 0, 0, 0,
+                           int(morton_order), int(max_steps))
+    ptr = lambda x: C.c_void_p(x.data_ptr())
+    torch.cuda.synchronize()
+    context.check(context._lib.dpa_advect_pathlines_device(
+        context.handle, field.handle, C.byref(opts), n, ptr(pos), ptr(t), ptr(rem), ptr(term),
+        None))
+    context.synchronize()
+    return PathlineResult(pos.cpu().numpy(), t.cpu().numpy(),
+                          rem.cpu().numpy().astype(np.uint64), term.cpu().numpy())

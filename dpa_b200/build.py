@@ -25,7 +25,8 @@ LIBRARY = PACKAGE / "libdpa_b200.so"
 PIPELINE = PACKAGE / "bin" / "dpa_pipeline"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SOURCES = ["capi.cu", "advect.cu", "emit.cu", "ftle.cu", "noalloc.cu", "serve.cu"]
+CUDA_SOURCES = ["capi.cu", "advect.cu", "advect_unsteady.cu", "emit.cu", "ftle.cu", "noalloc.cu",
+                "serve.cu"]
 
 
 def nvcc() -> str:
@@ -59,10 +60,17 @@ def build_library(force: bool = False, verbose_ptxas: bool = False) -> Path:
                     "-I", str(INCLUDE), "-I", str(CSRC), "--expt-relaxed-constexpr"]
     if verbose_ptxas:
         flags += ["-Xptxas", "-v"]
+    # The translation units compile in parallel (the advection kernel's
+    # instantiations dominate and are split across two of them).
+    from concurrent.futures import ThreadPoolExecutor
+    commands = []
     for src in sources:
         obj = build_dir / (src.stem + ".o")
-        _run([nvcc(), "-c", str(src), "-o", str(obj)] + flags)
+        commands.append([nvcc(), "-c", str(src), "-o", str(obj)] + flags)
         objects.append(str(obj))
+    with ThreadPoolExecutor(max_workers=min(len(commands), os.cpu_count() or 1)) as pool:
+        for f in [pool.submit(_run, c) for c in commands]:
+            f.result()
     tmp = LIBRARY.with_suffix(".so.tmp")
     _run([nvcc()] + ARCH + ["-shared", "-o", str(tmp)] + objects + ["-cudart", "static"])
     os.replace(tmp, LIBRARY)

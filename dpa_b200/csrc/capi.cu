@@ -110,10 +110,24 @@ int build_order(dpa_context* ctx, const dpa_field* field, const float* positions
   return DPA_OK;
 }
 
+// A time-varying field needs particle times, which only the pathline entry
+// points (and the request server) carry.
+int check_steady(dpa_context* ctx, const dpa_field* field) {
+  if (field->slices > 1)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT,
+                "the field varies in time: advect it with dpa_advect_pathlines_device");
+  return DPA_OK;
+}
+
 // Order (optional) + advection kernel over device arrays, no recording.
+// times (may be null for a steady field) are the particles' times.
 int advect_device_impl(dpa_context* ctx, const dpa_field* field, const dpa_advect_options* o,
                        uint64_t count, float* positions, uint64_t* remaining, uint8_t* termination,
-                       cudaStream_t s) {
+                       cudaStream_t s, float* times = nullptr) {
+  if (!times) {
+    const int st = check_steady(ctx, field);
+    if (st != DPA_OK) return st;
+  }
   if (count == 0) return DPA_OK;
   if (ctx->profiling) DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->events[0], s));
   const uint32_t* order = nullptr;
@@ -134,6 +148,7 @@ int advect_device_impl(dpa_context* ctx, const dpa_field* field, const dpa_advec
   a.positions = positions;
   a.remaining = remaining;
   a.termination = termination;
+  a.times = times;
   a.coefficients = dpa::make_step_coefficients(o->integrator, o->step_size);
   DPA_TRY_CUDA(ctx, dpa::launch_advect(field->view, a, o->integrator, false, s));
   ctx->launches += 1;
@@ -416,7 +431,8 @@ int dpa_integrator_from_name(const char* name, int32_t* integrator) {
 
 static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
                         const uint64_t shape[3], const float offset[3], const float spacing[3],
-                        int32_t storage, dpa_field** out) {
+                        int32_t storage, dpa_field** out, uint32_t slices = 1,
+                        float time_origin = 0.0f, float time_spacing = 0.0f) {
   if (!ctx || !out || !shape || !offset || !spacing)
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "NULL argument");
   *out = nullptr;
@@ -428,8 +444,14 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
     if (!(spacing[i] > 0.0f) || !std::isfinite(spacing[i]) || !std::isfinite(offset[i]))
       return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "spacing must be positive and finite");
   }
-  const uint64_t nodes = shape[0] * shape[1] * shape[2];
-  if (nodes > (1ull << 33)) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "field too large");
+  if (slices == 0) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "no time slices");
+  if (slices > 1 && (!(time_spacing > 0.0f) || !std::isfinite(time_spacing) ||
+                     !std::isfinite(time_origin)))
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "time spacing must be positive and finite");
+  const uint64_t slice_nodes = shape[0] * shape[1] * shape[2];
+  if (slice_nodes > (1ull << 33) || slice_nodes * slices > (1ull << 33))
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "field too large");
+  const uint64_t nodes = slice_nodes * slices;
   if (nodes && !xyzv) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "field data is NULL");
   return guarded(ctx, [&]() -> int {
     DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -474,6 +496,14 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
     v.stride1 = int32_t(shape[2]);
     v.storage = storage;
     v.pow2 = pow2 ? 1 : 0;
+    f->slices = slices;
+    f->time_origin = time_origin;
+    f->time_spacing = time_spacing;
+    v.slices = int32_t(slices);
+    v.slice_stride = int64_t(slice_nodes);
+    v.time_origin = time_origin;
+    v.time_spacing = slices > 1 ? time_spacing : 1.0f;
+    v.time_upper = float(int64_t(slices) - 1);
     *out = f;
     return DPA_OK;
   });
@@ -489,6 +519,25 @@ int dpa_field_create_device(dpa_context* ctx, const float* device_xyzv, const ui
                             const float offset[3], const float spacing[3], int32_t storage,
                             dpa_field** out) {
   return create_field(ctx, device_xyzv, true, shape, offset, spacing, storage, out);
+}
+
+int dpa_field_create_unsteady(dpa_context* ctx, const float* xyzv, const uint64_t shape[3],
+                              uint32_t slices, const float offset[3], const float spacing[3],
+                              float time_origin, float time_spacing, int32_t storage,
+                              dpa_field** out) {
+  if (ctx && slices < 2)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "a time-varying field needs 2 or more slices");
+  return create_field(ctx, xyzv, false, shape, offset, spacing, storage, out, slices, time_origin,
+                      time_spacing);
+}
+
+int dpa_field_time_info(const dpa_field* field, uint32_t* slices, float* time_origin,
+                        float* time_spacing) {
+  if (!field) return DPA_ERROR_INVALID_ARGUMENT;
+  if (slices) *slices = field->slices;
+  if (time_origin) *time_origin = field->time_origin;
+  if (time_spacing) *time_spacing = field->time_spacing;
+  return DPA_OK;
 }
 
 int dpa_field_destroy(dpa_context* ctx, dpa_field* field) {
@@ -521,6 +570,8 @@ int dpa_advect_round(dpa_context* ctx, const dpa_field* field, const dpa_advect_
   int st = check_options(ctx, options);
   if (st != DPA_OK) return st;
   if (!field || field->owner != ctx) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "bad field");
+  st = check_steady(ctx, field);
+  if (st != DPA_OK) return st;
   if (count && (!positions || !remaining))
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "positions or remaining is NULL");
   if (count > 0xffffffffull)
@@ -604,6 +655,28 @@ int dpa_advect_device(dpa_context* ctx, const dpa_field* field, const dpa_advect
     DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
     return advect_device_impl(ctx, field, options, count, device_positions, device_remaining,
                               device_termination, pick_stream(ctx, stream));
+  });
+}
+
+int dpa_advect_pathlines_device(dpa_context* ctx, const dpa_field* field,
+                                const dpa_advect_options* options, uint64_t count,
+                                float* device_positions, float* device_times,
+                                uint64_t* device_remaining, uint8_t* device_termination,
+                                void* stream) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  int st = check_options(ctx, options);
+  if (st != DPA_OK) return st;
+  if (options->record)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "dpa_advect_pathlines_device does not record");
+  if (!field || field->owner != ctx) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "bad field");
+  if (count && (!device_positions || !device_remaining || !device_times))
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "positions, times or remaining is NULL");
+  if (count > 0xffffffffull)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "at most 2^32-1 particles per call");
+  return guarded(ctx, [&]() -> int {
+    DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    return advect_device_impl(ctx, field, options, count, device_positions, device_remaining,
+                              device_termination, pick_stream(ctx, stream), device_times);
   });
 }
 
@@ -812,6 +885,8 @@ int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_adve
   if (options->record)
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "autotune measures calls without recording");
   if (!field || field->owner != ctx) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "bad field");
+  st = check_steady(ctx, field);
+  if (st != DPA_OK) return st;
   if (count == 0 || !device_positions || !device_remaining)
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "autotune needs particles");
   return guarded(ctx, [&]() -> int {
@@ -892,6 +967,8 @@ int dpa_advect_batch_device(dpa_context* ctx, const dpa_field* field,
   if (options->record)
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "batched launches do not record");
   if (!field || field->owner != ctx) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "bad field");
+  st = check_steady(ctx, field);
+  if (st != DPA_OK) return st;
   if (set_count && !set_offsets) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "set_offsets is NULL");
   for (uint64_t i = 0; i < set_count; ++i)
     if (set_offsets[i + 1] < set_offsets[i])
@@ -942,6 +1019,8 @@ int dpa_graph_create_advect(dpa_context* ctx, const dpa_field* field,
   if (st != DPA_OK) return st;
   if (options->record) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "graphs do not record");
   if (!field || field->owner != ctx) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "bad field");
+  st = check_steady(ctx, field);
+  if (st != DPA_OK) return st;
   if (count == 0 || count > 0xffffffffull || !device_positions || !device_remaining)
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "graphs need 1 to 2^32-1 particles");
   return guarded(ctx, [&]() -> int {

@@ -37,6 +37,13 @@ struct FieldView {
   float upper[3];        // n - 1: inside iff 0 <= (p - offset) / h < n - 1
   int32_t storage;       // dpa_storage
   int32_t pow2;          // every spacing is a power of two (division == product)
+  // Time-varying fields: `slices` grids of slice_stride nodes each, slice s
+  // at time time_origin + s * time_spacing; slices == 1 for a steady field.
+  int32_t slices;
+  int64_t slice_stride;
+  float time_origin;
+  float time_spacing;
+  float time_upper;      // slices - 1: inside iff 0 <= (t - t0) / dt < slices - 1
 };
 
 // Integrator id of the kernel instantiation shared by the reference's other

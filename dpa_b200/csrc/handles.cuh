@@ -119,5 +119,8 @@ struct dpa_field {
   float offset[3] = {0, 0, 0};
   float spacing[3] = {0, 0, 0};
   int32_t storage = DPA_STORAGE_F32;
+  uint32_t slices = 1;  // > 1: a time-varying field
+  float time_origin = 0.0f;
+  float time_spacing = 0.0f;
 };
 

@@ -17,6 +17,8 @@ struct AdvectArgs {
   float* positions;       // [count][3], updated in place
   uint64_t* remaining;    // [count], updated in place
   uint8_t* termination;   // [count] or null
+  float* times;           // [count] particle times, updated in place; required by
+                          // time-varying fields, optional (null) for steady ones
   StepCoefficients coefficients;
   uint64_t max_steps;                // step budget of this launch (~0: none)
   uint32_t claim;                    // order entries a warp claims at once
@@ -39,6 +41,7 @@ struct AdvectArgs {
 
 // Launch defaults: no step budget, 32-entry claims.
 inline void set_launch_defaults(AdvectArgs& a) {
+  a.times = nullptr;
   a.max_steps = ~0ull;
   a.claim = 32;
   a.blocks_per_sm = 0;
@@ -52,8 +55,13 @@ inline void set_launch_defaults(AdvectArgs& a) {
 cudaError_t launch_expand_ranges(const uint64_t* starts, const uint64_t* firsts, uint32_t ranges,
                                  uint64_t total, uint32_t* list, cudaStream_t stream);
 
+// Picks the kernel instantiation for the field (steady or time-varying,
+// storage, power-of-two spacing), the integrator and recording.
 cudaError_t launch_advect(const FieldView& f, const AdvectArgs& a, int integrator, bool record,
                           cudaStream_t stream);
+// The time-varying half of launch_advect (advect_unsteady.cu).
+cudaError_t launch_advect_unsteady(const FieldView& f, const AdvectArgs& a, int integrator,
+                                   bool record, cudaStream_t stream);
 
 // Resolves, outside any stream capture, what launch_advect looks up on its
 // first use of a kernel instantiation (its occupancy).

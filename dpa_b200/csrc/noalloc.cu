@@ -77,6 +77,9 @@ extern "C" int dpa_advect_device_no_alloc(dpa_context* ctx, const dpa_field* fie
   try {
     if (!options) return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT, "options is NULL");
     if (!field || field->owner != ctx) return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT, "bad field");
+    if (field->slices > 1)
+      return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT,
+                    "the field varies in time: advect it with dpa_advect_pathlines_device");
     if (options->record)
       return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT,
                     "dpa_advect_device_no_alloc does not record; use dpa_advect_round");

@@ -128,8 +128,10 @@ struct Corners {
 };
 
 template <int kStorage>
-__device__ __forceinline__ void gather(const FieldView& f, const int cell[3], Corners& k) {
-  const int64_t base = int64_t(cell[0]) * f.stride0 + int64_t(cell[1]) * f.stride1 + cell[2];
+__device__ __forceinline__ void gather(const FieldView& f, const int cell[3], Corners& k,
+                                       int64_t slice_base = 0) {
+  const int64_t base =
+      slice_base + int64_t(cell[0]) * f.stride0 + int64_t(cell[1]) * f.stride1 + cell[2];
   const int64_t s0 = f.stride0, s1 = f.stride1;
   float z[8];
   load_node<kStorage>(f.nodes, base, k.xy[0].x, k.xy[0].y, z[0]);
@@ -183,10 +185,11 @@ struct CellSampler {
   Corners corners;
   int cached[3] = {-1, -1, -1};
 
-  // Samples at p; returns false when p is outside the grid. The sample is
-  // returned as v01 = (v0, v1) and v2.
-  __device__ __forceinline__ bool sample(const FieldView& f, const Position& p, float2& v01,
-                                         float& v2) {
+  // Samples at p (a steady field: the time t is not used); returns false
+  // when p is outside the grid. The sample is returned as v01 = (v0, v1)
+  // and v2.
+  __device__ __forceinline__ bool sample(const FieldView& f, const Position& p, float /*t*/,
+                                         float2& v01, float& v2) {
     int cell[3];
     Weights w;
     if (!locate<kPow2>(f, p, cell, w)) return false;
@@ -201,6 +204,50 @@ struct CellSampler {
   }
 
   __device__ __forceinline__ void reset() { cached[0] = cached[1] = cached[2] = -1; }
+};
+
+// The time axis of a time-varying field, located by the spatial rule: slice
+// s = floor((t - t0) / dt) of the rounded quotient, weight fmod(t - t0, dt) / dt,
+// inside iff 0 <= s <= slices - 2. Returns the first node of slice s.
+__device__ __forceinline__ bool locate_time(const FieldView& f, float t, int64_t& slice_base,
+                                            float& w) {
+  const float a = __fsub_rn(t, f.time_origin);
+  const float q = __fdiv_rn(a, f.time_spacing);
+  if (!(q >= 0.0f && q < f.time_upper)) return false;
+  const float s = floorf(q);
+  w = weight_general(a, s, f.time_spacing);
+  slice_base = int64_t(s) * f.slice_stride;
+  return true;
+}
+
+// Sampler of a time-varying field: the trilinear samples of the two slices
+// around t at p, blended as (1 - w) * a + w * b per component. No corner
+// cache: the two slices' corners would not fit the register budget, and one
+// time window of a field is small enough to stay in L2.
+template <int kStorage, bool kPow2>
+struct TimeSampler {
+  __device__ __forceinline__ bool sample(const FieldView& f, const Position& p, float t,
+                                         float2& v01, float& v2) {
+    int cell[3];
+    Weights w;
+    if (!locate<kPow2>(f, p, cell, w)) return false;
+    int64_t slice = 0;
+    float wt = 0.0f;
+    if (!locate_time(f, t, slice, wt)) return false;
+    Corners c;
+    float2 a01, b01;
+    float a2, b2;
+    gather<kStorage>(f, cell, c, slice);
+    trilinear(c, w, a01, a2);
+    gather<kStorage>(f, cell, c, slice + f.slice_stride);
+    trilinear(c, w, b01, b2);
+    const float u = __fsub_rn(1.0f, wt);
+    v01 = lerp2(a01, b01, splat(u), splat(wt));
+    v2 = __fadd_rn(__fmul_rn(u, a2), __fmul_rn(wt, b2));
+    return true;
+  }
+
+  __device__ __forceinline__ void reset() {}
 };
 
 __device__ __forceinline__ bool is_zero(float2 v01, float v2) {
@@ -279,13 +326,15 @@ __device__ __forceinline__ void general_step(const GeneralCoefficients& g, float
 
 // One integrator step in place. The derivative of p0 is v2 and that of
 // (p2, p1) is (v0, v1) (particle_advector.cpp:369).
-template <int kIntegrator, int kStorage, bool kPow2>
+// t is the particle's time (used by time-varying fields only); the caller
+// advances it by dt after a step is taken.
+template <int kIntegrator, class Sampler>
 __device__ __forceinline__ int step(const FieldView& f, const StepCoefficients& k,
-                                   CellSampler<kStorage, kPow2>& sampler, Position& p,
+                                   Sampler& sampler, Position& p, float t,
                                    StepHistory& history) {
   float2 v01;
   float v2;
-  if (!sampler.sample(f, p, v01, v2)) return kStepOutOfBounds;
+  if (!sampler.sample(f, p, t, v01, v2)) return kStepOutOfBounds;
   if (is_zero(v01, v2)) return kStepZeroVelocity;
   if constexpr (kIntegrator == DPA_INTEGRATOR_EULER) {
     // odeint euler: x = 1 * x + dt * dxdt
@@ -308,13 +357,14 @@ __device__ __forceinline__ int step(const FieldView& f, const StepCoefficients& 
     Position x;
     x.p0 = __fadd_rn(p.p0, __fmul_rn(k.half, v2));
     x.p21 = add2(p.p21, mul2(splat(k.half), v01));
-    if (!sampler.sample(f, x, k2_01, k2_2)) return kStepOutOfBounds;
+    const float t_half = __fadd_rn(t, k.half), t_end = __fadd_rn(t, k.dt);
+    if (!sampler.sample(f, x, t_half, k2_01, k2_2)) return kStepOutOfBounds;
     x.p0 = __fadd_rn(p.p0, __fmul_rn(k.half, k2_2));
     x.p21 = add2(p.p21, mul2(splat(k.half), k2_01));
-    if (!sampler.sample(f, x, k3_01, k3_2)) return kStepOutOfBounds;
+    if (!sampler.sample(f, x, t_half, k3_01, k3_2)) return kStepOutOfBounds;
     x.p0 = __fadd_rn(p.p0, __fmul_rn(k.dt, k3_2));
     x.p21 = add2(p.p21, mul2(splat(k.dt), k3_01));
-    if (!sampler.sample(f, x, k4_01, k4_2)) return kStepOutOfBounds;
+    if (!sampler.sample(f, x, t_end, k4_01, k4_2)) return kStepOutOfBounds;
     p.p0 = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(p.p0, __fmul_rn(k.c0, v2)),
                                          __fmul_rn(k.c1, k2_2)),
                                __fmul_rn(k.c1, k3_2)),

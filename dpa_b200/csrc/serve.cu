@@ -100,7 +100,7 @@ struct active_request {
 
 struct response_storage {
   dpa_response r{};
-  std::vector<float> positions, vertices, colors, ftle;
+  std::vector<float> positions, times, vertices, colors, ftle;
   std::vector<uint64_t> remaining, indices64;
   std::vector<uint32_t> indices32;
   std::vector<uint8_t> termination;
@@ -115,8 +115,8 @@ struct dpa_server {
   cudaStream_t stream = nullptr;
 
   // Particle arena (per slot) and curve staging arena (per vertex).
-  DeviceBuffer positions, remaining, remaining_initial, termination, raw_offsets, kept_vertices,
-      kept_segments, curve_open, request_of, raw, in_flight;
+  DeviceBuffer positions, times, remaining, remaining_initial, termination, raw_offsets,
+      kept_vertices, kept_segments, curve_open, request_of, raw, in_flight;
   // Per tick.
   DeviceBuffer list, starts, firsts, work_counter;
   PinnedBuffer host_ranges, host_in_flight;
@@ -208,6 +208,9 @@ void dpa_server::upload(const active_request& a) {
                                cudaMemcpyHostToDevice, stream));
     std::vector<uint64_t> rem(n, q.iterations), raw_off;
     std::vector<uint32_t> owner(n, a.slot);
+    std::vector<float> start(n, q.start_time);
+    SERVER_TRY(cudaMemcpyAsync(times.as<float>() + first, start.data(), n * 4,
+                               cudaMemcpyHostToDevice, stream));
     SERVER_TRY(cudaMemcpyAsync(remaining.as<uint64_t>() + first, rem.data(), n * 8,
                                cudaMemcpyHostToDevice, stream));
     SERVER_TRY(cudaMemcpyAsync(remaining_initial.as<uint64_t>() + first, rem.data(), n * 8,
@@ -265,6 +268,7 @@ bool dpa_server::tick() {
     a.count = total;
     a.order = list.as<uint32_t>();
     a.positions = positions.as<float>();
+    a.times = times.as<float>();
     a.remaining = remaining.as<uint64_t>();
     a.termination = termination.as<uint8_t>();
     a.coefficients = dpa::make_step_coefficients(integrator, step_size);
@@ -295,10 +299,13 @@ void dpa_server::finish(active_request& a, response_storage& out) {
   const dpa_request& q = a.p.request;
   const uint64_t n = q.count, first = a.first;
   out.positions.resize(3 * n);
+  out.times.resize(n);
   out.remaining.resize(n);
   out.termination.resize(n);
   if (n) {
     SERVER_TRY(cudaMemcpyAsync(out.positions.data(), positions.as<float>() + 3 * first, n * 12,
+                               cudaMemcpyDeviceToHost, stream));
+    SERVER_TRY(cudaMemcpyAsync(out.times.data(), times.as<float>() + first, n * 4,
                                cudaMemcpyDeviceToHost, stream));
     SERVER_TRY(cudaMemcpyAsync(out.remaining.data(), remaining.as<uint64_t>() + first, n * 8,
                                cudaMemcpyDeviceToHost, stream));
@@ -419,6 +426,7 @@ void dpa_server::finish(active_request& a, response_storage& out) {
   r.user = q.user;
   r.count = n;
   r.positions = out.positions.data();
+  r.times = out.times.data();
   r.remaining = out.remaining.data();
   r.termination = out.termination.data();
   r.vertex_count = vertex_count;
@@ -516,11 +524,11 @@ int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_s
     }
     const uint64_t p = options->particle_capacity, v = options->vertex_capacity;
     cudaError_t e = cudaSuccess;
-    DeviceBuffer* per_slot[] = {&s->positions, &s->remaining, &s->remaining_initial,
+    DeviceBuffer* per_slot[] = {&s->positions, &s->times, &s->remaining, &s->remaining_initial,
                                 &s->termination, &s->raw_offsets, &s->kept_vertices,
                                 &s->kept_segments, &s->curve_open, &s->request_of};
-    const size_t bytes[] = {12, 8, 8, 1, 8, 4, 4, 1, 4};
-    for (size_t i = 0; i < 9 && e == cudaSuccess; ++i) e = per_slot[i]->reserve(p * bytes[i]);
+    const size_t bytes[] = {12, 4, 8, 8, 1, 8, 4, 4, 1, 4};
+    for (size_t i = 0; i < 10 && e == cudaSuccess; ++i) e = per_slot[i]->reserve(p * bytes[i]);
     if (e == cudaSuccess) e = s->raw.reserve(std::max<uint64_t>(v, 1) * 12);
     if (e == cudaSuccess) e = s->in_flight.reserve(4 * uint64_t(options->max_requests));
     if (e == cudaSuccess) e = s->work_counter.reserve(8);

@@ -17,7 +17,7 @@ import math
 
 import numpy as np
 
-from .advector import RegularGrid
+from .advector import RegularGrid, UnsteadyGrid
 
 ABC_A = math.sqrt(3.0)
 ABC_B = math.sqrt(2.0)
@@ -124,3 +124,37 @@ def linear(n: int, gradient: np.ndarray, constant, spacing=(1.0, 1.0, 1.0),
     xyz = offset.astype(np.float64) + idx * spacing.astype(np.float64)
     data = np.asarray(constant, np.float64) + xyz @ np.asarray(gradient, np.float64).T
     return RegularGrid.from_data(data.astype(np.float32), spacing, offset)
+
+
+def double_gyre_velocity(x, y, z, t, A=0.1, epsilon=0.25, omega=2.0 * math.pi / 10.0):
+    """Time-dependent double gyre on [0, 2] x [0, 1] (Shadden et al. 2005),
+    with an added vertical component w = 0.1 sin(pi z):
+    f(x, t) = a x^2 + b x, a = eps sin(wt), b = 1 - 2 eps sin(wt);
+    u = -pi A sin(pi f) cos(pi y), v = pi A cos(pi f) sin(pi y) df/dx."""
+    a = epsilon * np.sin(omega * t)
+    b = 1.0 - 2.0 * epsilon * np.sin(omega * t)
+    f = a * x * x + b * x
+    dfdx = 2.0 * a * x + b
+    u = -math.pi * A * np.sin(math.pi * f) * np.cos(math.pi * y)
+    v = math.pi * A * np.cos(math.pi * f) * np.sin(math.pi * y) * dfdx
+    w = 0.1 * np.sin(math.pi * z) + 0.0 * t
+    return u, v, w
+
+
+def double_gyre(shape=(128, 64, 64), slices: int = 32, period: float = 10.0, A=0.1,
+                epsilon=0.25) -> UnsteadyGrid:
+    """The double gyre sampled on [0, 2] x [0, 1] x [0, 1] with `slices` time
+    slices spanning one period [0, period] (slice spacing period / (slices - 1))."""
+    n = shape
+    h = np.array([2.0 / (n[0] - 1), 1.0 / (n[1] - 1), 1.0 / (n[2] - 1)], np.float32)
+    x = np.arange(n[0], dtype=np.float64)[:, None, None] * np.float64(h[0])
+    y = np.arange(n[1], dtype=np.float64)[None, :, None] * np.float64(h[1])
+    z = np.arange(n[2], dtype=np.float64)[None, None, :] * np.float64(h[2])
+    dt = np.float32(period / (slices - 1))
+    data = np.empty((slices,) + tuple(n) + (3,), np.float32)
+    for s in range(slices):
+        t = np.float64(np.float32(s) * dt)
+        u, v, w = double_gyre_velocity(x, y, z, t, A, epsilon, 2.0 * math.pi / period)
+        u, v, w = np.broadcast_arrays(u, v, w)
+        data[s] = _store_reversed(u, v, w)
+    return UnsteadyGrid.from_data(data, h, float(dt))

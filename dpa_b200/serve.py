@@ -26,6 +26,7 @@ class Result:
     queued: float
     admitted: float
     finished: float
+    times: np.ndarray | None = None  # each particle's time at its end
 
     @property
     def latency(self) -> float:
@@ -54,12 +55,13 @@ class Server:
 
     def submit(self, field_id: int, positions, iterations: int, integrator: str = "runge_kutta_4",
                step_size: float = 0.25, record: bool = False, index64: bool = False,
-               ftle: bool = False, seed_stride=(1.0, 1.0, 1.0)) -> int:
+               ftle: bool = False, seed_stride=(1.0, 1.0, 1.0), start_time: float = 0.0) -> int:
         pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
         req = N.Request(int(field_id), N.INTEGRATORS[integrator], float(np.float32(step_size)),
                         int(record), int(index64), int(ftle),
                         (C.c_float * 3)(*[float(v) for v in seed_stride]), pos.shape[0],
-                        pos.ctypes.data_as(C.POINTER(C.c_float)), int(iterations), None)
+                        pos.ctypes.data_as(C.POINTER(C.c_float)), int(iterations), None,
+                        float(np.float32(start_time)))
         rid = C.c_uint64()
         status = self._lib.dpa_server_submit(self.handle, C.byref(req), C.byref(rid))
         if status != N.DPA_OK:
@@ -91,9 +93,10 @@ class Server:
         if r.ftle:
             shape = tuple(int(s) for s in r.ftle_shape)
             ftle = np.ctypeslib.as_array(r.ftle, shape=(int(np.prod(shape)),)).reshape(shape).copy()
+        times = arr(r.times, (n,)).astype(np.float32) if (n and r.times) else np.zeros(0, np.float32)
         result = Result(int(r.id), int(r.status), pos, rem, term, vertices, colors, indices, ftle,
                         int(r.particle_steps), r.queued_seconds, r.admitted_seconds,
-                        r.finished_seconds)
+                        r.finished_seconds, times)
         self._lib.dpa_server_release(self.handle, r.id)
         self._index64.pop(r.id, None)
         return result

@@ -185,6 +185,24 @@ int dpa_field_destroy(dpa_context* ctx, dpa_field* field);
 int dpa_field_info(const dpa_field* field, uint64_t shape[3], float offset[3], float spacing[3],
                    int32_t* storage, uint64_t* device_bytes);
 
+/* A time-varying field (no counterpart in the reference, which advects
+ * steady fields): `slices` (>= 2) samples of one grid, slice s holding the
+ * field at time time_origin + s * time_spacing, in host memory as
+ * [slices][n0][n1][n2][3]. The velocity at (p, t) blends the trilinear samples
+ * of slices s and s + 1 at p as (1 - w) a + w b, where s = floor((t - t0) /
+ * dt) and w = fmod(t - t0, dt) / dt (the spatial rule on the time axis); a
+ * particle whose time leaves [t0, t0 + (slices - 1) dt) ends out of bounds.
+ * Advect it with dpa_advect_pathlines_device or the request server; the
+ * other advection calls refuse it. */
+int dpa_field_create_unsteady(dpa_context* ctx, const float* xyzv, const uint64_t shape[3],
+                              uint32_t slices, const float offset[3], const float spacing[3],
+                              float time_origin, float time_spacing, int32_t storage,
+                              dpa_field** out);
+
+/* slices = 1 (and zero times) for a steady field. */
+int dpa_field_time_info(const dpa_field* field, uint32_t* slices, float* time_origin,
+                        float* time_spacing);
+
 /* ---- advection --------------------------------------------------------------- */
 
 /* One advection round over host arrays: replaces particle_advector::
@@ -202,6 +220,18 @@ int dpa_advect_round(dpa_context* ctx, const dpa_field* field, const dpa_advect_
 int dpa_advect_device(dpa_context* ctx, const dpa_field* field, const dpa_advect_options* options,
                       uint64_t count, float* device_positions, uint64_t* device_remaining,
                       uint8_t* device_termination, void* stream);
+
+/* dpa_advect_device with a time per particle (device_times, float[count]),
+ * advanced by step_size for every step taken and updated in place: pathlines
+ * through a time-varying field (dpa_field_create_unsteady), or streamlines
+ * through a steady one with their times tracked. Four-sample RK4 samples its
+ * stages at t, t + dt/2 and t + dt; the other integrators sample at t. With
+ * max_steps a particle resumes at its stored time in a later call. */
+int dpa_advect_pathlines_device(dpa_context* ctx, const dpa_field* field,
+                                const dpa_advect_options* options, uint64_t count,
+                                float* device_positions, float* device_times,
+                                uint64_t* device_remaining, uint8_t* device_termination,
+                                void* stream);
 
 /* ---- batching, graphs and tuning (no counterpart in the reference) -------- */
 
@@ -282,6 +312,8 @@ typedef struct dpa_request {
   const float* positions;      /* host, count * 3; copied by dpa_server_submit */
   uint64_t    iterations;      /* per seed */
   void*       user;
+  float       start_time;      /* the seeds' time: pathlines through a time-varying
+                                  field start there (steady fields: tracked only) */
 } dpa_request;
 
 /* A finished request. Arrays are host memory owned by the server until
@@ -305,6 +337,7 @@ typedef struct dpa_response {
   double         queued_seconds;
   double         admitted_seconds;
   double         finished_seconds;
+  const float*   times;         /* count: each particle's time at its end */
 } dpa_response;
 
 typedef struct dpa_server_stats {

@@ -26,6 +26,12 @@ class Grid(C.Structure):
                 ("spacing", C.c_float * 3)]
 
 
+class UnsteadyGridC(C.Structure):
+    _fields_ = [("data", C.c_void_p), ("shape", C.c_uint64 * 3), ("slices", C.c_uint64),
+                ("offset", C.c_float * 3), ("spacing", C.c_float * 3),
+                ("time_origin", C.c_float), ("time_spacing", C.c_float)]
+
+
 _lib = None
 
 
@@ -50,6 +56,8 @@ def lib() -> C.CDLL:
         L.oracle_advect_round.argtypes = [P, C.c_int, C.c_float, C.c_uint64, P, P, P, P, C.c_int,
                                           C.c_uint64, P]
         L.oracle_advect_round.restype = C.c_int
+        L.oracle_advect_pathlines.argtypes = [P, C.c_int, C.c_float, C.c_uint64, P, P, P, P, P]
+        L.oracle_advect_pathlines.restype = C.c_int
         L.oracle_prune.argtypes = [P, C.c_uint64]
         L.oracle_prune.restype = C.c_uint64
         L.oracle_generate_indices.argtypes = [P, C.c_uint64, C.c_int, P]
@@ -231,3 +239,26 @@ def advect64_abc(A, B, Cc, lo, hi, step, positions, remaining):
                                    _ptr(rem), _ptr(term), _ptr(steps))
     assert rc == 0
     return RoundResult(pos, rem, term, steps)
+
+
+def advect_pathlines(grid, integrator: str, step: float, positions, times, remaining) -> RoundResult:
+    """Pathlines through a time-varying field (an object with data [S][n0][n1][n2][3],
+    offset, spacing, time_origin, time_spacing). The result's `steps` holds the
+    steps taken and its extra attribute `times` the final times."""
+    data = np.ascontiguousarray(grid.data, np.float32)
+    g = UnsteadyGridC(data.ctypes.data, (C.c_uint64 * 3)(*data.shape[1:4]), data.shape[0],
+                      (C.c_float * 3)(*np.asarray(grid.offset, np.float32)),
+                      (C.c_float * 3)(*np.asarray(grid.spacing, np.float32)),
+                      float(np.float32(grid.time_origin)), float(np.float32(grid.time_spacing)))
+    pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3).copy()
+    n = pos.shape[0]
+    t = np.broadcast_to(np.asarray(times, np.float32), (n,)).copy()
+    rem = np.broadcast_to(np.asarray(remaining, np.uint64), (n,)).copy()
+    term = np.zeros(n, np.uint8)
+    steps = np.zeros(n, np.uint64)
+    rc = lib().oracle_advect_pathlines(C.byref(g), INTEGRATOR_CODES[integrator], float(step), n,
+                                       _ptr(pos), _ptr(t), _ptr(rem), _ptr(term), _ptr(steps))
+    assert rc == 0, rc
+    res = RoundResult(pos, rem, term, steps)
+    res.times = t
+    return res

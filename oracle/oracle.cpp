@@ -279,19 +279,65 @@ void odeint_step(int integrator, float dt, const float* d, odeint_state& st, flo
 }
 
 // ---------------------------------------------------------------------------
+// The field a particle loop samples: the reference's steady regular_grid, or
+// a time-varying field (pathlines; no counterpart in the reference).
+// ---------------------------------------------------------------------------
+struct steady_field {
+  const oracle_grid& g;
+  bool contains(const float* p, float) const { return grid_contains(g, p); }
+  void interpolate(const float* p, float, float* out) const { grid_interpolate(g, p, out); }
+};
+
+// Slices of one grid at times t0 + s * dt. The time axis follows the spatial
+// rule of regular_grid.hpp:41-75: slice floor((t - t0) / dt) must lie in
+// [0, slices - 2], weight fmod(t - t0, dt) / dt, and the two slices' samples
+// blend as (1 - w) * a + w * b.
+struct unsteady_field {
+  const oracle_unsteady_grid& u;
+  oracle_grid slice(std::uint64_t s) const {
+    oracle_grid g;
+    g.data = u.data + s * u.shape[0] * u.shape[1] * u.shape[2] * 3;
+    for (int i = 0; i < 3; ++i) {
+      g.shape[i] = u.shape[i];
+      g.offset[i] = u.offset[i];
+      g.spacing[i] = u.spacing[i];
+    }
+    return g;
+  }
+  bool contains(const float* p, float t) const {
+    const float subscript = std::floor((t - u.time_origin) / u.time_spacing);
+    if (!(subscript >= 0.0f) || !(subscript <= static_cast<float>(u.slices - 2))) return false;
+    return grid_contains(slice(0), p);
+  }
+  void interpolate(const float* p, float t, float* out) const {
+    const float w = std::fmod(t - u.time_origin, u.time_spacing) / u.time_spacing;
+    const auto s = static_cast<std::uint64_t>(std::floor((t - u.time_origin) / u.time_spacing));
+    float a[3], b[3];
+    grid_interpolate(slice(s), p, a);
+    grid_interpolate(slice(s + 1), p, b);
+    for (int c = 0; c < 3; ++c) out[c] = (1.0f - w) * a[c] + w * b[c];
+  }
+};
+
+// ---------------------------------------------------------------------------
 // particle_advector::advect, one particle (particle_advector.cpp:325-396)
 // ---------------------------------------------------------------------------
-std::uint8_t advect_one(const oracle_grid& g, int integrator, const step_coefficients& k,
+// t (may be null: the time is then not tracked) is the particle's time, which
+// advances by dt with every step taken.
+template <class Field>
+std::uint8_t advect_one(const Field& g, int integrator, const step_coefficients& k,
                         float* pos, std::uint64_t* remaining, std::uint64_t* steps_out,
-                        float* curve /* null or curve_stride * 3 floats */) {
+                        float* curve /* null or curve_stride * 3 floats */,
+                        float* time = nullptr) {
+  float t = time ? *time : 0.0f;
   std::uint64_t iteration = 0;
   std::uint8_t reason = ORACLE_COMPLETE;
   odeint_state state;  // `auto integrator = integrator_;` per particle (:335)
   if (curve) std::memcpy(curve, pos, 3 * sizeof(float));
   for (; *remaining > 0; ++iteration, --*remaining) {
-    if (!grid_contains(g, pos)) { reason = ORACLE_OUT_OF_BOUNDS; break; }
+    if (!g.contains(pos, t)) { reason = ORACLE_OUT_OF_BOUNDS; break; }
     float v[3];
-    grid_interpolate(g, pos, v);
+    g.interpolate(pos, t, v);
     if (is_zero(v)) { reason = ORACLE_ZERO_VELOCITY; break; }
     float d[3];
     derivative_of(v, d);
@@ -309,21 +355,25 @@ std::uint8_t advect_one(const oracle_grid& g, int integrator, const step_coeffic
       // Four-sample RK4 (not part of the reference): stages at x,
       // x + dt/2 k1, x + dt/2 k2, x + dt k3; a stage outside the grid ends
       // the particle as out of bounds without taking the step.
+      // Stage times t + dt/2, t + dt/2 and t + dt.
       float k2[3], k3[3], k4[3], x[3], w[3];
+      const float t_half = t + k.half, t_end = t + k.dt;
       for (int c = 0; c < 3; ++c) x[c] = pos[c] + k.half * d[c];
-      if (!grid_contains(g, x)) { reason = ORACLE_OUT_OF_BOUNDS; break; }
-      grid_interpolate(g, x, w); derivative_of(w, k2);
+      if (!g.contains(x, t_half)) { reason = ORACLE_OUT_OF_BOUNDS; break; }
+      g.interpolate(x, t_half, w); derivative_of(w, k2);
       for (int c = 0; c < 3; ++c) x[c] = pos[c] + k.half * k2[c];
-      if (!grid_contains(g, x)) { reason = ORACLE_OUT_OF_BOUNDS; break; }
-      grid_interpolate(g, x, w); derivative_of(w, k3);
+      if (!g.contains(x, t_half)) { reason = ORACLE_OUT_OF_BOUNDS; break; }
+      g.interpolate(x, t_half, w); derivative_of(w, k3);
       for (int c = 0; c < 3; ++c) x[c] = pos[c] + k.dt * k3[c];
-      if (!grid_contains(g, x)) { reason = ORACLE_OUT_OF_BOUNDS; break; }
-      grid_interpolate(g, x, w); derivative_of(w, k4);
+      if (!g.contains(x, t_end)) { reason = ORACLE_OUT_OF_BOUNDS; break; }
+      g.interpolate(x, t_end, w); derivative_of(w, k4);
       for (int c = 0; c < 3; ++c)
         pos[c] = pos[c] + k.c0 * d[c] + k.c1 * k2[c] + k.c1 * k3[c] + k.c0 * k4[c];
     }
+    t = t + k.dt;
     if (curve) std::memcpy(curve + 3 * (iteration + 1), pos, 3 * sizeof(float));
   }
+  if (time) *time = t;
   if (curve) {
     float* t = curve + 3 * (iteration + 1);
     t[0] = t[1] = t[2] = kTerminal;
@@ -482,8 +532,29 @@ int oracle_advect_round(const oracle_grid* grid, int integrator, float step_size
   for (long long i = 0; i < static_cast<long long>(count); ++i) {
     float* curve = record ? raw_vertices + static_cast<uint64_t>(i) * curve_stride * 3 : nullptr;
     uint64_t taken = 0;
-    const uint8_t reason = advect_one(*grid, integrator, k, positions + 3 * i, remaining + i,
-                                      &taken, curve);
+    const uint8_t reason = advect_one(steady_field{*grid}, integrator, k, positions + 3 * i,
+                                      remaining + i, &taken, curve);
+    if (termination) termination[i] = reason;
+    if (steps) steps[i] = taken;
+  }
+  return 0;
+}
+
+int oracle_advect_pathlines(const oracle_unsteady_grid* grid, int integrator, float step_size,
+                            uint64_t count, float* positions, float* times, uint64_t* remaining,
+                            uint8_t* termination, uint64_t* steps) {
+  if (!grid || grid->slices < 2 || (count && (!positions || !times || !remaining))) return 1;
+  if (!((integrator >= ORACLE_EULER && integrator <= ORACLE_ADAMS_BASHFORTH_MOULTON_2) ||
+        integrator == ORACLE_RUNGE_KUTTA_4_TRUE))
+    return 2;
+  const step_coefficients k = make_coefficients(step_size);
+  const unsteady_field field{*grid};
+  const int threads = oracle_get_threads();
+#pragma omp parallel for schedule(dynamic, 1) num_threads(threads)
+  for (long long i = 0; i < static_cast<long long>(count); ++i) {
+    uint64_t taken = 0;
+    const uint8_t reason = advect_one(field, integrator, k, positions + 3 * i, remaining + i,
+                                      &taken, nullptr, times + i);
     if (termination) termination[i] = reason;
     if (steps) steps[i] = taken;
   }

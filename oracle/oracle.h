@@ -73,6 +73,26 @@ int oracle_advect_round(const oracle_grid* grid, int integrator, float step_size
                         uint8_t* termination, uint64_t* steps,
                         int record, uint64_t curve_stride, float* raw_vertices);
 
+/* A time-varying field: `slices` grids of one shape, slice s at time
+ * time_origin + s * time_spacing. Not part of the reference, which advects
+ * steady fields; the pathline rules restate the library's documented ones. */
+typedef struct oracle_unsteady_grid {
+  const float* data;      /* [slices][n0][n1][n2][3] */
+  uint64_t     shape[3];
+  uint64_t     slices;
+  float        offset[3];
+  float        spacing[3];
+  float        time_origin;
+  float        time_spacing;
+} oracle_unsteady_grid;
+
+/* Pathlines: oracle_advect_round's particle loop (no recording) with a time
+ * per particle, advanced by step_size per step; a particle whose time leaves
+ * the slices' span ends out of bounds. */
+int oracle_advect_pathlines(const oracle_unsteady_grid* grid, int integrator, float step_size,
+                            uint64_t count, float* positions, float* times, uint64_t* remaining,
+                            uint8_t* termination, uint64_t* steps);
+
 /* Removes invalid-sentinel vertices in place; returns the kept count
  * (particle_advector.cpp:402-408). */
 uint64_t oracle_prune(float* vertices, uint64_t vertex_count);
