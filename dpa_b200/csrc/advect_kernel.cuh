@@ -38,24 +38,34 @@ struct CurveCounter {
 // of one warp end after very different numbers of steps. A particle takes at
 // most a.max_steps steps per launch; one stopped by that budget alone is
 // reported as in flight and resumes in a later launch.
+//
+// Between hand-outs the warp runs stretches: every active lane steps until
+// one of the warp's particles stops, with one vote per step and a 32-bit step
+// counter per stretch (a stretch ends at 2^32 - 1 steps at the latest).
 template <int kIntegrator, int kStorage, bool kPow2, bool kRecord, bool kUnsteady>
 __global__ void __launch_bounds__(kAdvectBlock, kAdvectMinBlocks)
 advect_kernel(const FieldView f, const AdvectArgs a) {
   using Sampler = std::conditional_t<kUnsteady, TimeSampler<kStorage, kPow2>,
                                      CellSampler<kStorage, kPow2>>;
   constexpr unsigned kFull = 0xffffffffu;
+  // State touched only when particles are handed out or finish lives in
+  // shared memory, leaving the registers to the stepping loop: the warp's
+  // claim [next, end) of the order, and each lane's particle index.
+  __shared__ uint64_t claims[kAdvectBlock / 32][2];
+  __shared__ uint64_t particle[kAdvectBlock];
   const uint32_t claim = a.claim;
   const unsigned lane = threadIdx.x & 31u;
-  const unsigned lanes_below = (1u << lane) - 1u;
-
-  // Warp-uniform claim: entries [claim_next, claim_end) of the order.
-  uint64_t claim_next = 0, claim_end = 0;
+  uint64_t* const warp_claim = claims[threadIdx.x >> 5];
+  if (lane == 0) warp_claim[0] = warp_claim[1] = 0;
+  __syncwarp();
   bool exhausted = false;
 
   bool active = false;
-  uint64_t k = 0, remaining = 0, budget = 0, it = 0;
+  // rem: the particle's remaining iterations; left: steps it may still take
+  // in this launch (its remaining iterations or the launch's step budget).
+  uint64_t rem = 0, left = 0;
   Position p{0.0f, make_float2(0.0f, 0.0f)};
-  float* curve = nullptr;
+  float* curve = nullptr;  // the particle's last written vertex
   CurveCounter counter;
   Sampler sampler;
   StepHistory history{};
@@ -65,7 +75,8 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
     // Hand new particles to idle lanes.
     unsigned idle = __ballot_sync(kFull, !active);
     while (idle && !exhausted) {
-      if (claim_next == claim_end) {
+      uint64_t next = warp_claim[0], end = warp_claim[1];
+      if (next == end) {
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(a.work_counter, (unsigned long long)claim);
         base = __shfl_sync(kFull, base, 0);
@@ -73,37 +84,38 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
           exhausted = true;
           break;
         }
-        claim_next = base;
-        claim_end = base + claim < a.count ? base + claim : a.count;
+        next = base;
+        end = base + claim < a.count ? base + claim : a.count;
       }
-      const uint32_t left = uint32_t(claim_end - claim_next);
-      const uint32_t take = uint32_t(__popc(idle)) < left ? uint32_t(__popc(idle)) : left;
-      const uint32_t rank = __popc(idle & lanes_below);
-      // Lanes still in the idle set take entries claim_next + rank. (A lane
-      // that drew a finished particle earlier in this round is inactive but
-      // no longer idle, and must not take one again.)
+      const uint32_t avail = uint32_t(end - next);
+      const uint32_t take = uint32_t(__popc(idle)) < avail ? uint32_t(__popc(idle)) : avail;
+      const uint32_t rank = __popc(idle & ((1u << lane) - 1u));
+      // Lanes still in the idle set take entries next + rank. (A lane that
+      // drew a finished particle earlier in this round is inactive but no
+      // longer idle, and must not take one again.)
       const bool took = ((idle >> lane) & 1u) && rank < take;
       bool mine = took;
+      uint64_t k = 0;
       if (mine) {
-        const uint64_t t = claim_next + rank;
-        k = a.order ? a.order[t] : t;
+        const uint64_t e = next + rank;
+        k = a.order ? a.order[e] : e;
         // Serving: a finished particle stays finished.
         if (a.resume_only && a.termination[k] != DPA_TERMINATION_IN_FLIGHT) mine = false;
       }
       if (mine) {
+        particle[threadIdx.x] = k;
         p.p0 = a.positions[3 * k];
         p.p21 = make_float2(a.positions[3 * k + 2], a.positions[3 * k + 1]);
-        remaining = a.remaining[k];
+        rem = a.remaining[k];
         if (a.times) t = a.times[k];
-        budget = remaining < a.max_steps ? remaining : a.max_steps;
-        it = 0;
+        left = rem < a.max_steps ? rem : a.max_steps;
         sampler.reset();
         history.started = false;
         active = true;
         if constexpr (kRecord) {
           // A particle resumed from an earlier launch continues its curve
           // where that launch left it.
-          const uint64_t done = a.remaining_initial ? a.remaining_initial[k] - remaining : 0;
+          const uint64_t done = a.remaining_initial ? a.remaining_initial[k] - rem : 0;
           curve = a.raw_vertices + 3 * (a.raw_offsets[k] + done);
           counter = CurveCounter();
           if (done == 0) {
@@ -118,7 +130,12 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
           }
         }
       }
-      claim_next += take;
+      __syncwarp();
+      if (lane == 0) {
+        warp_claim[0] = next + take;
+        warp_claim[1] = end;
+      }
+      __syncwarp();
       // Every lane that took an entry leaves this round of hand-outs; one that
       // drew a finished particle (serving) stays inactive until the next.
       idle &= ~__ballot_sync(kFull, took);
@@ -128,51 +145,72 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
       continue;  // every lane drew a finished particle (serving): claim again
     }
 
-    if (active) {
-      int r = kStepTaken;
-      if (it < budget) {
+    // One stretch. Inactive lanes (the order ran out) only vote.
+    const uint64_t allowed = active ? left : 0;
+    const uint32_t limit = allowed < 0xffffffffull ? uint32_t(allowed) : 0xffffffffu;
+    uint32_t it = 0;
+    int r = kStepTaken;
+    bool stop = active && limit == 0;
+    while (!__any_sync(kFull, stop)) {
+      if (active) {
         r = step<kIntegrator>(f, a.coefficients, sampler, p, t, history);
         if (r == kStepTaken) {
           ++it;
-          t = __fadd_rn(t, a.coefficients.dt);
+          if constexpr (kUnsteady) t = __fadd_rn(t, a.coefficients.dt);
           if constexpr (kRecord) {
-            float* v = curve + 3 * it;
+            float* v = curve + 3 * uint64_t(it);
             v[0] = p.p0;
             v[1] = p.p21.y;
             v[2] = p.p21.x;
             counter.append(p.p0, p.p21.y, p.p21.x);
           }
+          stop = it >= limit;
+        } else {
+          stop = true;
         }
-      }
-      if (r != kStepTaken || it >= budget) {
-        const int reason = r == kStepOutOfBounds    ? DPA_TERMINATION_OUT_OF_BOUNDS
-                           : r == kStepZeroVelocity ? DPA_TERMINATION_ZERO_VELOCITY
-                           : it >= remaining        ? DPA_TERMINATION_COMPLETE
-                                                    : DPA_TERMINATION_IN_FLIGHT;
-        if constexpr (kRecord) {
-          if (reason != DPA_TERMINATION_IN_FLIGHT) {
-            float* v = curve + 3 * (it + 1);
-            v[0] = kTerminal;
-            v[1] = kTerminal;
-            v[2] = kTerminal;
-            counter.append(kTerminal, kTerminal, kTerminal);
-          } else {
-            a.curve_open[k] = counter.prev_open ? 1 : 0;
-          }
-          a.kept_vertices[k] = counter.kept;
-          a.kept_segments[k] = counter.segments;
-        }
-        a.positions[3 * k] = p.p0;
-        a.positions[3 * k + 1] = p.p21.y;
-        a.positions[3 * k + 2] = p.p21.x;
-        a.remaining[k] = remaining - it;
-        if (a.times) a.times[k] = t;
-        if (a.termination) a.termination[k] = uint8_t(reason);
-        if (a.in_flight && reason != DPA_TERMINATION_IN_FLIGHT)
-          atomicSub(a.in_flight + a.request_of[k], 1u);
-        active = false;
       }
     }
+    if (!active) continue;
+    rem -= it;
+    left -= it;
+    if constexpr (!kUnsteady) {
+      // A steady field's particles carry their time only when asked to; it
+      // advances by dt per step taken, rounded step by step as a
+      // time-varying field's does.
+      if (a.times)
+        for (uint32_t i = 0; i < it; ++i) t = __fadd_rn(t, a.coefficients.dt);
+    }
+    if constexpr (kRecord) curve += 3 * uint64_t(it);
+    // A particle that only reached the end of a stretch carries on.
+    if (!stop || (r == kStepTaken && left > 0)) continue;
+
+    const uint64_t k = particle[threadIdx.x];
+    const int reason = r == kStepOutOfBounds    ? DPA_TERMINATION_OUT_OF_BOUNDS
+                       : r == kStepZeroVelocity ? DPA_TERMINATION_ZERO_VELOCITY
+                       : rem == 0               ? DPA_TERMINATION_COMPLETE
+                                                : DPA_TERMINATION_IN_FLIGHT;
+    if constexpr (kRecord) {
+      if (reason != DPA_TERMINATION_IN_FLIGHT) {
+        float* v = curve + 3;
+        v[0] = kTerminal;
+        v[1] = kTerminal;
+        v[2] = kTerminal;
+        counter.append(kTerminal, kTerminal, kTerminal);
+      } else {
+        a.curve_open[k] = counter.prev_open ? 1 : 0;
+      }
+      a.kept_vertices[k] = counter.kept;
+      a.kept_segments[k] = counter.segments;
+    }
+    a.positions[3 * k] = p.p0;
+    a.positions[3 * k + 1] = p.p21.y;
+    a.positions[3 * k + 2] = p.p21.x;
+    a.remaining[k] = rem;
+    if (a.times) a.times[k] = t;
+    if (a.termination) a.termination[k] = uint8_t(reason);
+    if (a.in_flight && reason != DPA_TERMINATION_IN_FLIGHT)
+      atomicSub(a.in_flight + a.request_of[k], 1u);
+    active = false;
   }
 }
 

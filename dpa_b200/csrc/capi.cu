@@ -61,6 +61,20 @@ bool is_power_of_two(float h) {
          std::isnormal(1.0f / h);
 }
 
+// Axes on which the kernels may locate with q = fma(p, 1 / h, -offset / h):
+// h a power of two in [2^-20, 2^20] and offset zero or at least 2^-100 in
+// magnitude. Then offset / h is an exact float and the fma's one rounding of
+// (p - offset) / h equals the reference's rounded p - offset scaled exactly by
+// 1 / h: whenever the scaled quotient could fall below the normal range,
+// p - offset is itself exact (p is then within a factor of two of offset, or
+// offset is zero).
+bool exact_scaled_axis(float h, float offset) {
+  if (!is_power_of_two(h) || h < std::ldexp(1.0f, -20) || h > std::ldexp(1.0f, 20)) return false;
+  if (offset != 0.0f && !(std::fabs(offset) >= std::ldexp(1.0f, -100))) return false;
+  const float scaled = offset * (1.0f / h);
+  return std::isfinite(scaled) && double(scaled) * double(h) == double(offset);
+}
+
 cudaStream_t pick_stream(dpa_context* ctx, void* stream) {
   return stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
 }
@@ -481,7 +495,7 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
       f->shape[i] = shape[i];
       f->offset[i] = offset[i];
       f->spacing[i] = spacing[i];
-      pow2 = pow2 && is_power_of_two(spacing[i]);
+      pow2 = pow2 && exact_scaled_axis(spacing[i], offset[i]);
     }
     dpa::FieldView& v = f->view;
     v.nodes = f->nodes.ptr;
@@ -490,6 +504,7 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
       v.offset[i] = offset[i];
       v.spacing[i] = spacing[i];
       v.inv_spacing[i] = 1.0f / spacing[i];
+      v.scaled_offset[i] = offset[i] * v.inv_spacing[i];
       v.upper[i] = float(int64_t(shape[i]) - 1);
     }
     v.stride0 = int64_t(shape[1]) * int64_t(shape[2]);

@@ -33,10 +33,14 @@ struct FieldView {
   int32_t stride1;     // n2
   float offset[3];
   float spacing[3];
-  float inv_spacing[3];  // exact reciprocals, used only when pow2 is set
-  float upper[3];        // n - 1: inside iff 0 <= (p - offset) / h < n - 1
-  int32_t storage;       // dpa_storage
-  int32_t pow2;          // every spacing is a power of two (division == product)
+  float inv_spacing[3];    // exact reciprocals, used only when pow2 is set
+  float scaled_offset[3];  // offset / spacing, exact; used only when pow2 is set
+  float upper[3];          // n - 1: inside iff 0 <= (p - offset) / h < n - 1
+  int32_t storage;         // dpa_storage
+  // Every spacing is a power of two in [2^-20, 2^20] and every offset is zero
+  // or at least 2^-100 in magnitude: (p - offset) / h is then one rounding of
+  // p / h - offset / h, and fmod(p - offset, h) / h is q - floor(q).
+  int32_t pow2;
   // Time-varying fields: `slices` grids of slice_stride nodes each, slice s
   // at time time_origin + s * time_spacing; slices == 1 for a steady field.
   int32_t slices;

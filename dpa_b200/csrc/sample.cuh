@@ -7,6 +7,8 @@
 // same rounding as the reference's FP32 build.
 #pragma once
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace dpa {
@@ -35,15 +37,21 @@ __device__ __forceinline__ void load_node(const void* nodes, int64_t index, floa
   }
 }
 
-// Two FP32 lanes, each rounded on its own with the scalar __fadd_rn /
-// __fmul_rn, which the compiler never contracts into an FMA. (sm_100's packed
-// f32x2 add and multiply are contracted into packed FMAs by the compiler even
-// with explicit .rn rounding, so they cannot reproduce the reference's
-// separately rounded products and sums.)
+// Two FP32 lanes. Products use sm_100's packed multiply (FMUL2), whose
+// lanes round exactly as __fmul_rn does. Sums that may take such a product
+// as an operand stay scalar (__fadd_rn): the compiler fuses a packed multiply
+// feeding a packed add into one packed FMA even when both carry explicit
+// round-to-nearest, and the fused result differs from the reference's
+// separately rounded product and sum. sum2 is the packed add for operands
+// that are never products.
 __device__ __forceinline__ float2 add2(float2 a, float2 b) {
   return make_float2(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y));
 }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) {
+__device__ __forceinline__ float2 sum2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+// Two scalar products, for lerps whose operands would need extra register
+// moves to form the pairs a packed multiply reads.
+__device__ __forceinline__ float2 mul2_scalar(float2 a, float2 b) {
   return make_float2(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y));
 }
 __device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
@@ -69,9 +77,9 @@ struct Weights {
 // is inside iff 0 <= s <= n - 2 on every axis (regular_grid::contains), which
 // for any float q (NaN included) is 0 <= q < n - 1.
 //
-// Power-of-two spacing: a / h is exact, and so is fmod(a, h) / h = q - s, whose
-// difference is representable; the sign of a zero weight follows q as fmod's
-// follows a.
+// Power-of-two spacing (FieldView::pow2): q is one FMA of the exact p / h and
+// offset / h, and fmod(a, h) / h = q - s, whose difference is representable;
+// the sign of a zero weight follows q as fmod's follows a.
 //
 // Other spacings: the rounded quotient is either the true integer quotient N
 // or N + 1 (only when a / h lies within half an ulp below N + 1, so that
@@ -87,15 +95,21 @@ __device__ __forceinline__ float weight_general(float a, float s, float h) {
 template <bool kPow2>
 __device__ __forceinline__ bool locate(const FieldView& f, const Position& p, int cell[3],
                                        Weights& w) {
-  const float a0 = __fsub_rn(p.p0, f.offset[0]);
-  const float2 a21 = add2(p.p21, neg2(make_float2(f.offset[2], f.offset[1])));
   float q0, q2, q1;
+  float a0 = 0.0f;
+  float2 a21 = make_float2(0.0f, 0.0f);
   if constexpr (kPow2) {
-    q0 = __fmul_rn(a0, f.inv_spacing[0]);
-    const float2 q21 = mul2(a21, make_float2(f.inv_spacing[2], f.inv_spacing[1]));
+    // q = p / h - offset / h in one rounding: p / h and offset / h are exact,
+    // so this is the reference's rounded (p - offset) scaled by 1 / h.
+    q0 = __fmaf_rn(p.p0, f.inv_spacing[0], -f.scaled_offset[0]);
+    const float2 q21 =
+        __ffma2_rn(p.p21, make_float2(f.inv_spacing[2], f.inv_spacing[1]),
+                   make_float2(-f.scaled_offset[2], -f.scaled_offset[1]));
     q2 = q21.x;
     q1 = q21.y;
   } else {
+    a0 = __fsub_rn(p.p0, f.offset[0]);
+    a21 = sum2(p.p21, neg2(make_float2(f.offset[2], f.offset[1])));
     q0 = __fdiv_rn(a0, f.spacing[0]);
     q2 = __fdiv_rn(a21.x, f.spacing[2]);
     q1 = __fdiv_rn(a21.y, f.spacing[1]);
@@ -105,7 +119,7 @@ __device__ __forceinline__ bool locate(const FieldView& f, const Position& p, in
   const float s0 = floorf(q0), s1 = floorf(q1), s2 = floorf(q2);
   if constexpr (kPow2) {
     w.w0 = copysignf(__fsub_rn(q0, s0), q0);
-    const float2 d = add2(make_float2(q2, q1), neg2(make_float2(s2, s1)));
+    const float2 d = sum2(make_float2(q2, q1), neg2(make_float2(s2, s1)));
     w.w21 = make_float2(copysignf(d.x, q2), copysignf(d.y, q1));
   } else {
     w.w0 = weight_general(a0, s0, f.spacing[0]);
@@ -118,20 +132,50 @@ __device__ __forceinline__ bool locate(const FieldView& f, const Position& p, in
   return inside;
 }
 
-// The eight corners of one cell, corner j = dx * 4 + dy * 2 + dz (the
-// permute_for order of permute_for.hpp:12-34), arranged for packed lerps:
-// xy[j] = (v0, v1) of corner j, and the v2 components paired as
-// (corner 0, corner 4), (1, 5), (2, 6), (3, 7).
-struct Corners {
+// (1 - w) * lo + w * hi per lane, every operation rounded on its own.
+__device__ __forceinline__ float2 lerp2(float2 lo, float2 hi, float2 one_minus_w, float2 w) {
+  return add2(mul2(one_minus_w, lo), mul2(w, hi));
+}
+
+// The eight corners of one cell are corner j = dx * 4 + dy * 2 + dz (the
+// permute_for order of permute_for.hpp:12-34). Two register layouts of them
+// serve the trilinear reduction of regular_grid.hpp:71-73 (axis 2, then 1,
+// then 0, with c[j] = (1 - w) * c[2j] + w * c[2j+1]); both give the same
+// bits, and each storage takes the one that measured faster on the B200.
+//
+// CornerNodes (F32 nodes): xy[j] = (v0, v1) of corner j, and the v2
+// components paired as (corner 0, corner 4), (1, 5), (2, 6), (3, 7). A
+// 16-byte node load lands (v0, v1) in a register pair as it is, and the
+// lerps multiply in scalar: packed products would need the weights
+// duplicated into pairs, and the extra registers cost more than the packed
+// multiply saves at F32's load width.
+struct CornerNodes {
   float2 xy[8];
   float2 z04, z15, z26, z37;
 };
 
+// CornerEdges (F16 / BF16 nodes): z[e][c] = (component c of corner 2e,
+// component c of corner 2e + 1), the two ends of edge e = dx * 2 + dy along
+// axis 2, formed as the 16-bit values are widened. Each lerp is one packed
+// multiply of (lo, hi) by the weight pair (1 - w, w) and one scalar sum.
+struct CornerEdges {
+  float2 z[4][3];
+};
+
 template <int kStorage>
-__device__ __forceinline__ void gather(const FieldView& f, const int cell[3], Corners& k,
+using CornersOf =
+    std::conditional_t<kStorage == DPA_STORAGE_F32, CornerNodes, CornerEdges>;
+
+template <int kStorage>
+__device__ __forceinline__ int64_t cell_base(const FieldView& f, const int cell[3],
+                                             int64_t slice_base) {
+  return slice_base + int64_t(cell[0]) * f.stride0 + int64_t(cell[1]) * f.stride1 + cell[2];
+}
+
+template <int kStorage>
+__device__ __forceinline__ void gather(const FieldView& f, const int cell[3], CornerNodes& k,
                                        int64_t slice_base = 0) {
-  const int64_t base =
-      slice_base + int64_t(cell[0]) * f.stride0 + int64_t(cell[1]) * f.stride1 + cell[2];
+  const int64_t base = cell_base<kStorage>(f, cell, slice_base);
   const int64_t s0 = f.stride0, s1 = f.stride1;
   float z[8];
   load_node<kStorage>(f.nodes, base, k.xy[0].x, k.xy[0].y, z[0]);
@@ -148,33 +192,67 @@ __device__ __forceinline__ void gather(const FieldView& f, const int cell[3], Co
   k.z37 = make_float2(z[3], z[7]);
 }
 
-// (1 - w) * lo + w * hi per lane, every operation rounded on its own.
-__device__ __forceinline__ float2 lerp2(float2 lo, float2 hi, float2 one_minus_w, float2 w) {
-  return add2(mul2(one_minus_w, lo), mul2(w, hi));
+template <int kStorage>
+__device__ __forceinline__ void gather(const FieldView& f, const int cell[3], CornerEdges& k,
+                                       int64_t slice_base = 0) {
+  const int64_t base = cell_base<kStorage>(f, cell, slice_base);
+  const int64_t s0 = f.stride0, s1 = f.stride1;
+  const int64_t edge[4] = {base, base + s1, base + s0, base + s0 + s1};
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    float lo[3], hi[3];
+    load_node<kStorage>(f.nodes, edge[e], lo[0], lo[1], lo[2]);
+    load_node<kStorage>(f.nodes, edge[e] + 1, hi[0], hi[1], hi[2]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) k.z[e][c] = make_float2(lo[c], hi[c]);
+  }
 }
 
-// Trilinear reduction of regular_grid.hpp:71-73: axis 2, then 1, then 0, with
-// c[j] = (1 - w) * c[2j] + w * c[2j+1]. Components 0 and 1 travel as one pair;
-// component 2 pairs the reductions of the x0 and x1 halves of the cell.
-__device__ __forceinline__ void trilinear(const Corners& k, const Weights& w, float2& v01,
+__device__ __forceinline__ void trilinear(const CornerNodes& k, const Weights& w, float2& v01,
                                           float& v2) {
-  const float2 one = splat(1.0f);
-  const float2 t21 = add2(one, neg2(w.w21));
+  const float2 t21 = sum2(splat(1.0f), neg2(w.w21));
   const float t0 = __fsub_rn(1.0f, w.w0);
   const float2 W2 = splat(w.w21.x), T2 = splat(t21.x);
   const float2 W1 = splat(w.w21.y), T1 = splat(t21.y);
   const float2 W0 = splat(w.w0), T0 = splat(t0);
-  const float2 e0 = lerp2(k.xy[0], k.xy[1], T2, W2);
-  const float2 e1 = lerp2(k.xy[2], k.xy[3], T2, W2);
-  const float2 e2 = lerp2(k.xy[4], k.xy[5], T2, W2);
-  const float2 e3 = lerp2(k.xy[6], k.xy[7], T2, W2);
-  const float2 f0 = lerp2(e0, e1, T1, W1);
-  const float2 f1 = lerp2(e2, e3, T1, W1);
-  v01 = lerp2(f0, f1, T0, W0);
-  const float2 e02 = lerp2(k.z04, k.z15, T2, W2);  // (e0, e2) of component 2
-  const float2 e13 = lerp2(k.z26, k.z37, T2, W2);  // (e1, e3)
-  const float2 f01 = lerp2(e02, e13, T1, W1);      // (f0, f1)
+  auto lerp = [](float2 lo, float2 hi, float2 t, float2 u) {
+    return add2(mul2_scalar(t, lo), mul2_scalar(u, hi));
+  };
+  const float2 e0 = lerp(k.xy[0], k.xy[1], T2, W2);
+  const float2 e1 = lerp(k.xy[2], k.xy[3], T2, W2);
+  const float2 e2 = lerp(k.xy[4], k.xy[5], T2, W2);
+  const float2 e3 = lerp(k.xy[6], k.xy[7], T2, W2);
+  const float2 f0 = lerp(e0, e1, T1, W1);
+  const float2 f1 = lerp(e2, e3, T1, W1);
+  v01 = lerp(f0, f1, T0, W0);
+  const float2 e02 = lerp(k.z04, k.z15, T2, W2);  // (e0, e2) of component 2
+  const float2 e13 = lerp(k.z26, k.z37, T2, W2);  // (e1, e3)
+  const float2 f01 = lerp(e02, e13, T1, W1);      // (f0, f1)
   v2 = __fadd_rn(__fmul_rn(t0, f01.x), __fmul_rn(w.w0, f01.y));
+}
+
+// (1 - w) * lo + w * hi for the pair lohi = (lo, hi) and tw = (1 - w, w).
+__device__ __forceinline__ float lerp_pair(float2 lohi, float2 tw) {
+  const float2 m = mul2(tw, lohi);
+  return __fadd_rn(m.x, m.y);
+}
+
+__device__ __forceinline__ void trilinear(const CornerEdges& k, const Weights& w, float2& v01,
+                                          float& v2) {
+  const float2 tw2 = make_float2(__fsub_rn(1.0f, w.w21.x), w.w21.x);
+  const float2 tw1 = make_float2(__fsub_rn(1.0f, w.w21.y), w.w21.y);
+  const float2 tw0 = make_float2(__fsub_rn(1.0f, w.w0), w.w0);
+  float v[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float e0 = lerp_pair(k.z[0][c], tw2), e1 = lerp_pair(k.z[1][c], tw2);
+    const float e2 = lerp_pair(k.z[2][c], tw2), e3 = lerp_pair(k.z[3][c], tw2);
+    const float f0 = lerp_pair(make_float2(e0, e1), tw1);
+    const float f1 = lerp_pair(make_float2(e2, e3), tw1);
+    v[c] = lerp_pair(make_float2(f0, f1), tw0);
+  }
+  v01 = make_float2(v[0], v[1]);
+  v2 = v[2];
 }
 
 // A per-thread cache of the current cell's corners: a particle usually stays
@@ -182,7 +260,7 @@ __device__ __forceinline__ void trilinear(const Corners& k, const Weights& w, fl
 // whether the corners came from the cache or from memory.
 template <int kStorage, bool kPow2>
 struct CellSampler {
-  Corners corners;
+  CornersOf<kStorage> corners;
   int cached[3] = {-1, -1, -1};
 
   // Samples at p (a steady field: the time t is not used); returns false
@@ -234,7 +312,7 @@ struct TimeSampler {
     int64_t slice = 0;
     float wt = 0.0f;
     if (!locate_time(f, t, slice, wt)) return false;
-    Corners c;
+    CornersOf<kStorage> c;
     float2 a01, b01;
     float a2, b2;
     gather<kStorage>(f, cell, c, slice);
@@ -242,7 +320,7 @@ struct TimeSampler {
     gather<kStorage>(f, cell, c, slice + f.slice_stride);
     trilinear(c, w, b01, b2);
     const float u = __fsub_rn(1.0f, wt);
-    v01 = lerp2(a01, b01, splat(u), splat(wt));
+    v01 = add2(mul2_scalar(splat(u), a01), mul2_scalar(splat(wt), b01));
     v2 = __fadd_rn(__fmul_rn(u, a2), __fmul_rn(wt, b2));
     return true;
   }
