@@ -611,6 +611,7 @@ def run_gpu(a):
         "kernel_ms": statistics.mean(kernel_ms), "order_ms": statistics.mean(order_ms),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
+                     "dram_achieved": traffic / kernel_s / 1e9 if traffic else None,
                      "peak_source": peak_src,
                      "algorithmic_bytes": f"{BYTES_PER_STEP[a.storage]} B per particle-step "
                                           f"(8 corners x 3 x {BYTES_PER_STEP[a.storage] // 24} B)"
