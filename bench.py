@@ -46,6 +46,11 @@ def parse_args():
     p.add_argument("--steps", type=int, default=30)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="dpa_b200", choices=["dpa_b200", "reference"])
+    p.add_argument("--workload", default="throughput", choices=["throughput", "ftle", "recording"],
+                   help="throughput: the headline configuration (curl noise 256^3, 1M seeds x "
+                        "2000 steps, end positions); ftle: ABC + noise 256^3, 128^3 lattice x "
+                        "250 steps, then FTLE; recording: ABC 64^3, 4096 seeds x 1000 steps, "
+                        "curves with uint32 indices")
     p.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
     p.add_argument("--integrator", default="runge_kutta_4")
     p.add_argument("--n", type=int, default=256)
@@ -644,8 +649,242 @@ def run_gpu(a):
     return 0
 
 
+SECONDARY = {
+    # workload: field, seeds, iterations, step, what a step does
+    "ftle": "ABC flow + 5 % smoothed perturbation (sigma 3, seed 2) on 256^3 over [0, 2 pi]^3, "
+            "a 128^3 seed lattice (seed_generation_stride 2), runge_kutta_4 (one field sample "
+            "per step), step 0.02, 250 iterations, then the FTLE of the flow map",
+    "recording": "ABC flow on 64^3 over [0, 2 pi]^3, 4096 uniform seeds (seed 0) in the domain, "
+                 "runge_kutta_4 (one field sample per step), step 0.01, 1000 iterations, curve "
+                 "recording with uint32 indices and angular-velocity colors",
+}
+
+
+def secondary_inputs(a, device):
+    import math
+    from dpa_b200 import fields, seeds
+    if a.workload == "ftle":
+        grid = fields.abc_perturbed(256, 0.05, 3.0, 2, device=device)
+        offset, size = seeds.seed_box(grid)
+        parts = seeds.generate(offset, size, (grid.spacing * np.float32(2)).astype(np.float32), 250)
+        return grid, parts.position, 250, 0.02
+    grid = fields.abc(64)
+    offset, size = seeds.seed_box(grid)
+    parts = seeds.generate_random(offset, size, 4096, 1000, aabb=([0, 0, 0], [2 * math.pi] * 3),
+                                  seed=0)
+    return grid, parts.position, 1000, 0.01
+
+
+def run_secondary(a):
+    """The FTLE and recording configurations: device-timed steps through the
+    device entry points (FTLE) or the host round with its curve (recording),
+    in the same JSON layout as the headline workload."""
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if a.impl == "reference":
+        if rank != 0:
+            return 0
+        grid, pos, iterations, step = secondary_inputs(a, "cuda" if _cuda_available() else None)
+        from oracle import binding as ob
+        ob.build()
+        threads = os.cpu_count() or 1
+        ob.set_threads(threads)
+        og = ob.OracleGrid.of(grid)
+        values = []
+        sample = pos
+        if a.workload == "ftle":  # a seeded random sample of the lattice, ~5 s of work
+            sample = pos[np.sort(np.random.default_rng(11).choice(len(pos), 200_000, False))]
+        for i in range(a.warmup + a.steps):
+            t0 = time.perf_counter()
+            r = ob.advect_round(og, a.integrator, step, sample,
+                                np.full(len(sample), iterations, np.uint64),
+                                record=a.workload == "recording")
+            dt = time.perf_counter() - t0
+            if i >= a.warmup:
+                values.append(float(np.sum(r.steps)) / dt)
+        value = statistics.mean(values)
+        desc = (f"{len(sample)} of the {len(pos)} seeds at full {iterations} iterations per step; "
+                "oracle/oracle.cpp, OpenMP dynamic schedule standing in for TBB")
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+            "n_gpus": world, "steps": a.steps, "warmup": a.warmup, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": {"workload": SECONDARY[a.workload]},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": desc},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}), flush=True)
+        return 0
+
+    import ctypes as C
+    import torch
+    import dpa_b200
+    from dpa_b200 import ParticleAdvector, Particles
+    from dpa_b200 import _native as N
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    grid, pos, iterations, step = secondary_inputs(a, "cuda")
+    n = pos.shape[0]
+    ctx = dpa_b200.Context(local)
+    lib = ctx._lib
+    field = ctx.field(grid, a.storage)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    clocks = ClockSampler(local)
+    out = {"metric": METRIC, "unit": UNIT, "n_gpus": 1, "steps": a.steps, "warmup": a.warmup,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic",
+           "config": {"workload": SECONDARY[a.workload], "storage": a.storage,
+                      "l2": "256 MiB buffer written between timed steps (L2 flush)"}}
+    launches0 = C.c_uint64()
+    ctx.check(lib.dpa_context_launch_count(ctx.handle, C.byref(launches0)))
+    if a.workload == "ftle":
+        p0 = torch.from_numpy(pos).cuda()
+        r0 = torch.full((n,), iterations, dtype=torch.int64, device="cuda")
+        p, r = torch.empty_like(p0), torch.empty_like(r0)
+        term = torch.empty(n, dtype=torch.uint8, device="cuda")
+        stride = (C.c_float * 3)(2.0, 2.0, 2.0)
+        shape = (C.c_uint64 * 3)()
+        ftle = torch.empty(128 ** 3, dtype=torch.float32, device="cuda")
+        opts = N.AdvectOptions(N.INTEGRATORS[a.integrator], float(np.float32(step)), 0, 0, 0, 1)
+        ctx.check(lib.dpa_context_set_profiling(ctx.handle, 1))
+        kernel_ms, ftle_ms, total = [], [], 0.0
+
+        def one_step():
+            p.copy_(p0)
+            r.copy_(r0)
+            ctx.check(lib.dpa_advect_device(ctx.handle, field.handle, C.byref(opts), n,
+                                            C.c_void_p(p.data_ptr()), C.c_void_p(r.data_ptr()),
+                                            C.c_void_p(term.data_ptr()),
+                                            C.c_void_p(stream.cuda_stream)))
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            ctx.check(lib.dpa_ftle_estimate_device(
+                ctx.handle, field.handle, stride, iterations, float(np.float32(step)), n,
+                C.c_void_p(p0.data_ptr()), C.c_void_p(p.data_ptr()), 0,
+                C.c_void_p(ftle.data_ptr()), shape, C.c_void_p(stream.cuda_stream)))
+            e1.record(stream)
+            return e0, e1
+
+        for _ in range(a.warmup):
+            flush.fill_(1)
+            one_step()
+        torch.cuda.synchronize()
+        ctx.check(lib.dpa_context_launch_count(ctx.handle, C.byref(launches0)))
+        clocks.start()
+        time.sleep(0.3)  # the sampler's first readings
+        for _ in range(a.steps):
+            flush.fill_(2)
+            start = torch.cuda.Event(enable_timing=True)
+            end = torch.cuda.Event(enable_timing=True)
+            start.record(stream)
+            e0, e1 = one_step()
+            end.record(stream)
+            end.synchronize()
+            total += start.elapsed_time(end)
+            o, k = C.c_float(), C.c_float()
+            ctx.check(lib.dpa_context_last_timing(ctx.handle, C.byref(o), C.byref(k)))
+            kernel_ms.append(k.value)
+            ftle_ms.append(e0.elapsed_time(e1))
+        out["clocks"] = clocks.stop()
+        steps_taken = float(np.sum(iterations - r.cpu().numpy()))
+        ms = total / a.steps
+        kern = statistics.mean(kernel_ms)
+        # End to end: the host entry points (dpa_advect_round, dpa_ftle_estimate)
+        # with pinned host buffers.
+        hp = torch.empty((n, 3), dtype=torch.float32, pin_memory=True).numpy()
+        hr = torch.empty(n, dtype=torch.int64, pin_memory=True).numpy().view(np.uint64)
+        ht = torch.empty(n, dtype=torch.uint8, pin_memory=True).numpy()
+        hf = torch.empty(128 ** 3, dtype=torch.float32, pin_memory=True).numpy()
+        hsh = (C.c_uint64 * 3)()
+
+        def e2e_once():
+            hp[:] = pos
+            hr[:] = iterations
+            t0 = time.perf_counter()
+            ctx.check(lib.dpa_advect_round(ctx.handle, field.handle, C.byref(opts), n,
+                                           hp.ctypes.data_as(C.c_void_p),
+                                           hr.ctypes.data_as(C.c_void_p),
+                                           ht.ctypes.data_as(C.c_void_p), N.CURVE_SINK(), None))
+            ctx.check(lib.dpa_ftle_estimate(ctx.handle, field.handle, stride, iterations,
+                                            float(np.float32(step)), n,
+                                            pos.ctypes.data_as(C.c_void_p),
+                                            hp.ctypes.data_as(C.c_void_p), 0,
+                                            hf.ctypes.data_as(C.c_void_p), hsh))
+            return time.perf_counter() - t0
+
+        e2e_once()
+        e2e = statistics.mean([e2e_once() for _ in range(3)])
+        out.update({
+            "value": steps_taken / (ms / 1e3), "ms_per_step": ms,
+            "particle_steps_per_step": steps_taken, "kernel_ms": kern,
+            "ftle_ms": statistics.mean(ftle_ms),
+            "e2e": {"value": steps_taken / e2e, "unit": UNIT,
+                    "h2d_bytes_per_step": n * (12 + 8) + n * 24,
+                    "d2h_bytes_per_step": n * (12 + 8 + 1) + 128 ** 3 * 4,
+                    "call": "dpa_advect_round + dpa_ftle_estimate with pinned host buffers"},
+        })
+        algorithmic = BYTES_PER_STEP[a.storage] * steps_taken + STATE_BYTES * n
+    else:
+        adv = ParticleAdvector(ctx, n, "none", a.integrator, step, False, True)
+        parts = Particles.create(pos, iterations)
+        for _ in range(a.warmup):
+            adv.advect(field, parts)
+        torch.cuda.synchronize()
+        ctx.check(lib.dpa_context_launch_count(ctx.handle, C.byref(launches0)))
+        clocks.start()
+        time.sleep(0.3)  # the sampler's first readings
+        times = []
+        for _ in range(a.steps):
+            flush.fill_(2)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = adv.advect(field, parts)
+            times.append(time.perf_counter() - t0)
+        out["clocks"] = clocks.stop()
+        curve = res.integral_curves[0]
+        steps_taken = float(np.sum(iterations - res.inactive_particles.remaining_iterations
+                                   .astype(np.int64)))
+        ms = statistics.mean(times) * 1e3
+        vertices = int(curve.vertices.shape[0])
+        out.update({
+            "value": steps_taken / (ms / 1e3), "ms_per_step": ms,
+            "particle_steps_per_step": steps_taken,
+            "curve": {"vertices": vertices, "indices": int(curve.indices.size),
+                      "index_dtype": str(curve.indices.dtype)},
+            "e2e": {"value": steps_taken / (ms / 1e3), "unit": UNIT,
+                    "h2d_bytes_per_step": n * (12 + 8),
+                    "d2h_bytes_per_step": n * (12 + 8 + 1) + vertices * 16 +
+                                          int(curve.indices.nbytes),
+                    "call": "ParticleAdvector.advect -> dpa_advect_round with recording "
+                            "(host buffers, curve chunks through the sink); the timed step "
+                            "is this end-to-end call"},
+        })
+        algorithmic = None
+    launches1 = C.c_uint64()
+    ctx.check(lib.dpa_context_launch_count(ctx.handle, C.byref(launches1)))
+    out["gpu_launches"] = int(launches1.value - launches0.value)
+    peak, peak_src = measured_peak_hbm()
+    if algorithmic is not None:
+        kernel_s = out["kernel_ms"] / 1e3
+        achieved = algorithmic / kernel_s / 1e9
+        out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                           "frac": achieved / peak, "traffic": None, "peak_source": peak_src,
+                           "algorithmic_bytes": f"{BYTES_PER_STEP[a.storage]} B per "
+                                                f"particle-step + {STATE_BYTES} B per particle",
+                           "kernel": "advect_kernel (CUDA events around its launch)"}
+    print(json.dumps(out), flush=True)
+    field.close()
+    ctx.close()
+    return 0
+
+
 def main():
     a = parse_args()
+    if a.workload != "throughput":
+        return run_secondary(a)
     if a.impl == "reference":
         return run_reference(a)
     return run_gpu(a)

@@ -8,79 +8,126 @@ namespace dpa {
 
 namespace {
 
-// Interleaves the low 4 bits of v with two zero bits between them.
-__device__ __forceinline__ uint32_t spread4(uint32_t v) {
-  v &= 0xfu;
-  v = (v | (v << 4)) & 0x0c3u;
-  v = (v | (v << 2)) & 0x249u;
-  return v;
+// Interleaves the low 6 bits of v with two zero bits between them.
+__device__ __forceinline__ uint32_t spread6(uint32_t v) {
+  uint32_t r = 0;
+#pragma unroll
+  for (int b = 0; b < 6; ++b) r |= ((v >> b) & 1u) << (3 * b);
+  return r;
 }
 
 // Processing-order bucket of a particle: the Morton code of its start cell
-// on a resolution^3 coarsening of the grid (resolution <= 16, so at most 4096
-// buckets), or kOrderBuckets for particles that start outside the grid.
+// on a resolution^3 coarsening of the grid, below buckets = p^3 for p the
+// power of two >= resolution (<= 64), or `buckets` for particles that start
+// outside the grid.
 __device__ __forceinline__ uint32_t order_bucket(const FieldView& f, const float* p,
-                                                 uint32_t resolution) {
+                                                 uint32_t resolution, uint32_t buckets) {
   uint32_t c[3];
 #pragma unroll
   for (int i = 0; i < 3; ++i) {
     const float q = (p[i] - f.offset[i]) * (1.0f / f.spacing[i]);
-    if (!(q >= 0.0f && q < f.upper[i])) return kOrderBuckets;
+    if (!(q >= 0.0f && q < f.upper[i])) return buckets;
     c[i] = uint32_t(floorf(q)) * resolution / uint32_t(f.n[i]);
   }
-  return (spread4(c[0]) << 2) | (spread4(c[1]) << 1) | spread4(c[2]);
+  return (spread6(c[0]) << 2) | (spread6(c[1]) << 1) | spread6(c[2]);
 }
 
-__global__ void order_clear_kernel(uint32_t* counts) {
-  for (int i = threadIdx.x; i <= kOrderBuckets; i += blockDim.x) counts[i] = 0;
-}
-
+// Bucket ids and their counts. Lanes of a warp that share a bucket (seeds are
+// often dense) add to its counter once.
 __global__ void order_histogram_kernel(const FieldView f, const float* positions, uint64_t count,
-                                       uint16_t* buckets, uint32_t* counts, uint32_t resolution) {
-  __shared__ uint32_t local[kOrderBuckets + 1];
-  for (int i = threadIdx.x; i <= kOrderBuckets; i += blockDim.x) local[i] = 0;
-  __syncthreads();
-  for (uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; t < count;
-       t += uint64_t(gridDim.x) * blockDim.x) {
-    const uint32_t b = order_bucket(f, positions + 3 * t, resolution);
-    buckets[t] = uint16_t(b);
-    atomicAdd(&local[b], 1u);
+                                       uint32_t* ids, uint32_t* counts, uint32_t resolution,
+                                       uint32_t buckets) {
+  for (uint64_t base = uint64_t(blockIdx.x) * blockDim.x; base < count;
+       base += uint64_t(gridDim.x) * blockDim.x) {
+    const uint64_t t = base + threadIdx.x;
+    const bool live = t < count;
+    const unsigned mask = __ballot_sync(0xffffffffu, live);
+    if (!live) continue;
+    const uint32_t b = order_bucket(f, positions + 3 * t, resolution, buckets);
+    ids[t] = b;
+    const unsigned same = __match_any_sync(mask, b);
+    if ((threadIdx.x & 31u) == unsigned(__ffs(same) - 1))
+      atomicAdd(&counts[b], uint32_t(__popc(same)));
   }
-  __syncthreads();
-  for (int i = threadIdx.x; i <= kOrderBuckets; i += blockDim.x)
-    if (local[i]) atomicAdd(&counts[i], local[i]);
 }
 
-// Exclusive scan of the bucket counts in one block; counts become cursors.
-__global__ void __launch_bounds__(1024) order_scan_kernel(uint32_t* counts) {
-  constexpr int kPer = (kOrderBuckets + 1 + 1023) / 1024;
-  __shared__ uint32_t sums[1024];
-  uint32_t v[kPer];
-  uint32_t total = 0;
+// Exclusive scan of the counts in tiles of kScanTile entries: tile sums,
+// a scan of the sums, then each tile's scan plus its prefix. 256 threads,
+// four consecutive entries each.
+constexpr uint32_t kScanTile = 1024;
+
+__device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t v, uint32_t* warp_sums,
+                                                         uint32_t* total) {
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  uint32_t x = v;
 #pragma unroll
-  for (int j = 0; j < kPer; ++j) {
-    const int i = threadIdx.x * kPer + j;
-    v[j] = i <= kOrderBuckets ? counts[i] : 0u;
-    total += v[j];
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= unsigned(o)) x += y;
   }
-  sums[threadIdx.x] = total;
+  if (lane == 31) warp_sums[warp] = x;
   __syncthreads();
-  for (int off = 1; off < 1024; off <<= 1) {
-    const uint32_t add = threadIdx.x >= off ? sums[threadIdx.x - off] : 0u;
-    __syncthreads();
-    sums[threadIdx.x] += add;
-    __syncthreads();
+  uint32_t before = 0, all = 0;
+  for (unsigned w = 0; w < blockDim.x / 32; ++w) {
+    if (w < warp) before += warp_sums[w];
+    all += warp_sums[w];
   }
-  uint32_t run = sums[threadIdx.x] - total;
+  *total = all;
+  return before + x - v;
+}
+
+__device__ __forceinline__ void load_tile(const uint32_t* counts, uint32_t n, uint32_t first,
+                                          uint32_t v[4]) {
 #pragma unroll
-  for (int j = 0; j < kPer; ++j) {
-    const int i = threadIdx.x * kPer + j;
-    if (i <= kOrderBuckets) counts[i] = run;
+  for (int j = 0; j < 4; ++j) {
+    const uint32_t i = first + 4 * threadIdx.x + j;
+    v[j] = i < n ? counts[i] : 0u;
+  }
+}
+
+__global__ void __launch_bounds__(256) order_tile_sums_kernel(const uint32_t* counts, uint32_t n,
+                                                              uint32_t* tile_sums) {
+  __shared__ uint32_t warp_sums[8];
+  uint32_t v[4];
+  load_tile(counts, n, blockIdx.x * kScanTile, v);
+  uint32_t total = 0;
+  block_exclusive_scan(v[0] + v[1] + v[2] + v[3], warp_sums, &total);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// One block: the exclusive scan of up to 256 * 4 tile sums, in place.
+__global__ void __launch_bounds__(256) order_scan_sums_kernel(uint32_t* tile_sums, uint32_t tiles) {
+  __shared__ uint32_t warp_sums[8];
+  uint32_t v[4];
+  load_tile(tile_sums, tiles, 0, v);
+  uint32_t total = 0;
+  uint32_t run = block_exclusive_scan(v[0] + v[1] + v[2] + v[3], warp_sums, &total);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const uint32_t i = 4 * threadIdx.x + j;
+    if (i < tiles) tile_sums[i] = run;
     run += v[j];
   }
 }
 
-__global__ void order_scatter_kernel(const uint16_t* buckets, uint64_t count, uint32_t* cursors,
+__global__ void __launch_bounds__(256) order_scan_tiles_kernel(uint32_t* counts, uint32_t n,
+                                                               const uint32_t* tile_prefix) {
+  __shared__ uint32_t warp_sums[8];
+  uint32_t v[4];
+  const uint32_t first = blockIdx.x * kScanTile;
+  load_tile(counts, n, first, v);
+  uint32_t total = 0;
+  uint32_t run = tile_prefix[blockIdx.x] +
+                 block_exclusive_scan(v[0] + v[1] + v[2] + v[3], warp_sums, &total);
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const uint32_t i = first + 4 * threadIdx.x + j;
+    if (i < n) counts[i] = run;
+    run += v[j];
+  }
+}
+
+__global__ void order_scatter_kernel(const uint32_t* buckets, uint64_t count, uint32_t* cursors,
                                      uint32_t* order) {
   const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= count) return;
@@ -149,16 +196,24 @@ cudaError_t prepare_advect(const FieldView& f, int integrator, bool record) {
 }
 
 cudaError_t launch_order(const FieldView& f, const float* positions, uint64_t count,
-                         uint16_t* buckets, uint32_t* counts, uint32_t* order, cudaStream_t stream,
+                         uint32_t* ids, uint32_t* counts, uint32_t* order, cudaStream_t stream,
                          uint32_t resolution) {
   if (count == 0) return cudaSuccess;
-  if (resolution < 1 || resolution > 16) resolution = 16;
-  order_clear_kernel<<<1, 1024, 0, stream>>>(counts);
+  if (resolution < 1 || resolution > kOrderMaxResolution) resolution = kOrderDefaultResolution;
+  uint32_t p = 1;
+  while (p < resolution) p *= 2;
+  const uint32_t buckets = p * p * p;
+  const uint32_t n = buckets + 1;  // the last counts the particles outside the grid
+  const uint32_t tiles = (n + kScanTile - 1) / kScanTile;
+  uint32_t* tile_sums = counts + kOrderBuckets + 1;
+  DPA_CUDA_TRY(cudaMemsetAsync(counts, 0, n * sizeof(uint32_t), stream));
   const uint64_t blocks = std::min<uint64_t>((count + 255) / 256, 4 * 148);
-  order_histogram_kernel<<<unsigned(blocks), 256, 0, stream>>>(f, positions, count, buckets, counts,
-                                                               resolution);
-  order_scan_kernel<<<1, 1024, 0, stream>>>(counts);
-  order_scatter_kernel<<<unsigned((count + 255) / 256), 256, 0, stream>>>(buckets, count, counts,
+  order_histogram_kernel<<<unsigned(blocks), 256, 0, stream>>>(f, positions, count, ids, counts,
+                                                               resolution, buckets);
+  order_tile_sums_kernel<<<tiles, 256, 0, stream>>>(counts, n, tile_sums);
+  order_scan_sums_kernel<<<1, 256, 0, stream>>>(tile_sums, tiles);
+  order_scan_tiles_kernel<<<tiles, 256, 0, stream>>>(counts, n, tile_sums);
+  order_scatter_kernel<<<unsigned((count + 255) / 256), 256, 0, stream>>>(ids, count, counts,
                                                                            order);
   return cudaGetLastError();
 }

@@ -113,10 +113,10 @@ int build_order(dpa_context* ctx, const dpa_field* field, const float* positions
                 cudaStream_t stream, const uint32_t** order) {
   *order = nullptr;
   if (count < 2) return DPA_OK;
-  DPA_TRY_CUDA(ctx, ctx->keys.reserve(count * 2));
+  DPA_TRY_CUDA(ctx, ctx->keys.reserve(count * 4));
   DPA_TRY_CUDA(ctx, ctx->values.reserve(count * 4));
-  DPA_TRY_CUDA(ctx, ctx->sort_temp.reserve((dpa::kOrderBuckets + 1) * 4));
-  DPA_TRY_CUDA(ctx, dpa::launch_order(field->view, positions, count, ctx->keys.as<uint16_t>(),
+  DPA_TRY_CUDA(ctx, ctx->sort_temp.reserve(dpa::kOrderCountsSize * 4));
+  DPA_TRY_CUDA(ctx, dpa::launch_order(field->view, positions, count, ctx->keys.as<uint32_t>(),
                                       ctx->sort_temp.as<uint32_t>(), ctx->values.as<uint32_t>(),
                                       stream, ctx->tuning.order));
   ctx->launches += dpa::kOrderLaunches;
@@ -873,8 +873,8 @@ int dpa_context_set_tuning(dpa_context* ctx, const dpa_tuning* tuning) {
   if (!ctx || !tuning) return DPA_ERROR_INVALID_ARGUMENT;
   if (tuning->claim < 1 || tuning->claim > 4096)
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "claim must be in [1, 4096]");
-  if (tuning->order > 16)
-    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "order resolution must be in [0, 16]");
+  if (tuning->order > dpa::kOrderMaxResolution)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "order resolution must be in [0, 64]");
   ctx->tuning.claim = tuning->claim;
   ctx->tuning.blocks_per_sm = tuning->blocks_per_sm;
   ctx->tuning.order = tuning->order;
@@ -931,7 +931,7 @@ int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_adve
     int rc = DPA_OK;
     const uint32_t claims[] = {16, 32, 64, 128};
     const uint32_t grids[] = {0, 3, 2};
-    const uint32_t orders[] = {16, 8, 0};
+    const uint32_t orders[] = {64, 16, 0};
     for (uint32_t order : orders)
       for (uint32_t grid : grids)
         for (uint32_t claim : claims) {
@@ -1042,9 +1042,9 @@ int dpa_graph_create_advect(dpa_context* ctx, const dpa_field* field,
     DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
     // Everything the launch sequence allocates or looks up, before capture.
-    DPA_TRY_CUDA(ctx, ctx->keys.reserve(count * 2));
+    DPA_TRY_CUDA(ctx, ctx->keys.reserve(count * 4));
     DPA_TRY_CUDA(ctx, ctx->values.reserve(count * 4));
-    DPA_TRY_CUDA(ctx, ctx->sort_temp.reserve((dpa::kOrderBuckets + 1) * 4));
+    DPA_TRY_CUDA(ctx, ctx->sort_temp.reserve(dpa::kOrderCountsSize * 4));
     DPA_TRY_CUDA(ctx, ctx->work_counter.reserve(sizeof(unsigned long long)));
     DPA_TRY_CUDA(ctx, dpa::prepare_advect(field->view, options->integrator, false));
     DPA_TRY_CUDA(ctx, cudaStreamSynchronize(s));

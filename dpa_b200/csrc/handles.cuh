@@ -73,10 +73,10 @@ using dpa::PinnedBuffer;
 
 // Launch parameters an autotuner may change per context.
 struct dpa_tuning_state {
-  uint32_t claim = 32;        // order entries a warp claims at once
+  uint32_t claim = 16;        // order entries a warp claims at once
   uint32_t blocks_per_sm = 0; // persistent grid: 0 = as many as fit
-  uint32_t order = 16;        // processing order: Morton buckets of an order^3
-                              // coarsening of the grid (1..16); 0: input order
+  uint32_t order = 64;        // processing order: Morton buckets of an order^3
+                              // coarsening of the grid (1..64); 0: input order
 };
 
 struct dpa_context {

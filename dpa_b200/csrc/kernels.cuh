@@ -39,11 +39,11 @@ struct AdvectArgs {
   unsigned int* in_flight;            // per request
 };
 
-// Launch defaults: no step budget, 32-entry claims.
+// Launch defaults: no step budget, 16-entry claims.
 inline void set_launch_defaults(AdvectArgs& a) {
   a.times = nullptr;
   a.max_steps = ~0ull;
-  a.claim = 32;
+  a.claim = 16;
   a.blocks_per_sm = 0;
   a.resume_only = false;
   a.request_of = nullptr;
@@ -68,14 +68,20 @@ cudaError_t launch_advect_unsteady(const FieldView& f, const AdvectArgs& a, int 
 cudaError_t prepare_advect(const FieldView& f, int integrator, bool record);
 
 // Processing order: a counting sort of the particles by the Morton code of
-// their start cell on a 16^3 coarsening of the grid (four kernels). Within a
-// bucket the order is arbitrary; results never depend on processing order.
-constexpr int kOrderBuckets = 4096;
-constexpr int kOrderLaunches = 4;
+// their start cell on a resolution^3 coarsening of the grid (a memset and
+// five kernels). Within a bucket the order is arbitrary; results never depend
+// on processing order. ids holds count bucket ids; counts holds
+// kOrderCountsSize counters (the buckets of the finest resolution, one for
+// particles outside the grid, and the scan's tile sums).
+constexpr uint32_t kOrderMaxResolution = 64;
+constexpr uint32_t kOrderDefaultResolution = 64;
+constexpr uint32_t kOrderBuckets = kOrderMaxResolution * kOrderMaxResolution * kOrderMaxResolution;
+constexpr uint32_t kOrderCountsSize = kOrderBuckets + 1 + (kOrderBuckets + 1 + 1023) / 1024;
+constexpr int kOrderLaunches = 5;
 
 cudaError_t launch_order(const FieldView& f, const float* positions, uint64_t count,
-                         uint16_t* buckets, uint32_t* counts, uint32_t* order, cudaStream_t stream,
-                         uint32_t resolution = 16);
+                         uint32_t* ids, uint32_t* counts, uint32_t* order, cudaStream_t stream,
+                         uint32_t resolution = kOrderDefaultResolution);
 
 // Particle-steps each seed set took: sum over [offsets[s], offsets[s+1]) of
 // remaining_in - remaining_out.

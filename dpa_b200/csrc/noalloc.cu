@@ -10,7 +10,7 @@
 // takes it from a fixed array compiled into the library instead.
 //
 // The array below is a file-scope __device__ array of kScratchBytes (about
-// 6.3 MiB). Every GPU on which the library's code is loaded holds its own copy
+// 9 MiB). Every GPU on which the library's code is loaded holds its own copy
 // until the process exits. Host code cannot use the name g_scratch as a device
 // address (on the host it names a host-side stand-in), so the device address
 // is looked up once per device with cudaGetSymbolAddress, with that device
@@ -31,9 +31,9 @@ constexpr size_t round_up(size_t n) { return (n + kAlign - 1) / kAlign * kAlign;
 constexpr size_t kCounterOffset = 0;
 constexpr size_t kCountsOffset = kAlign;
 constexpr size_t kOrderOffset =
-    kCountsOffset + round_up(size_t(dpa::kOrderBuckets + 1) * sizeof(uint32_t));
+    kCountsOffset + round_up(size_t(dpa::kOrderCountsSize) * sizeof(uint32_t));
 constexpr size_t kBucketsOffset = kOrderOffset + round_up(kMaxParticles * sizeof(uint32_t));
-constexpr size_t kScratchBytes = kBucketsOffset + round_up(kMaxParticles * sizeof(uint16_t));
+constexpr size_t kScratchBytes = kBucketsOffset + round_up(kMaxParticles * sizeof(uint32_t));
 
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
@@ -112,7 +112,7 @@ extern "C" int dpa_advect_device_no_alloc(dpa_context* ctx, const dpa_field* fie
       // left in the shared array does not matter.
       uint32_t* counts = reinterpret_cast<uint32_t*>(scratch + kCountsOffset);
       uint32_t* order_out = reinterpret_cast<uint32_t*>(scratch + kOrderOffset);
-      uint16_t* buckets = reinterpret_cast<uint16_t*>(scratch + kBucketsOffset);
+      uint32_t* buckets = reinterpret_cast<uint32_t*>(scratch + kBucketsOffset);
       e = dpa::launch_order(field->view, device_positions, count, buckets, counts, order_out, s);
       if (e != cudaSuccess) return refuse_cuda(ctx, e, "ordering kernels");
       order = order_out;

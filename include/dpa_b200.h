@@ -263,7 +263,7 @@ typedef struct dpa_tuning {
   uint32_t claim;          /* processing-order entries a warp takes per atomic claim */
   uint32_t blocks_per_sm;  /* persistent grid blocks per SM; 0 = as many as fit */
   uint32_t order;          /* processing order: Morton buckets of a order^3 coarsening
-                              of the grid (1..16), 0 = input order */
+                              of the grid (1..64), 0 = input order */
   float    measured_ms;    /* dpa_autotune_advect: time of the chosen setting */
 } dpa_tuning;
 
@@ -271,7 +271,7 @@ int dpa_context_set_tuning(dpa_context* ctx, const dpa_tuning* tuning);
 int dpa_context_get_tuning(const dpa_context* ctx, dpa_tuning* tuning);
 
 /* Times the candidate settings (claim 16..128, 2 to all resident blocks per SM,
- * order 16 / 8 / off) on copies of the first min(count, 4,194,304) of the
+ * order 64 / 16 / off) on copies of the first min(count, 4,194,304) of the
  * given device particles, each advanced at most sample_steps steps (0: its
  * whole remaining budget, capped by options->max_steps), keeps the fastest in
  * the context and returns it in best (may be NULL). The processing order pays
@@ -372,7 +372,7 @@ int dpa_server_destroy(dpa_server* server);
  * and cudaFree may synchronize the whole device and stall other streams.
  * Same inputs, outputs and results as dpa_advect_device (recording is not
  * offered); the ordering scratch comes from a fixed device array inside the
- * library (about 6.3 MiB, held by every GPU on which the library's code is
+ * library (about 9 MiB, held by every GPU on which the library's code is
  * loaded until the process exits) instead of cudaMalloc. At most
  * DPA_NO_ALLOC_MAX_PARTICLES particles per call; more is rejected with
  * DPA_ERROR_INVALID_ARGUMENT. The first call on a device resolves the array's
