@@ -434,10 +434,28 @@ def serving_run(a, ctx, rate=200.0):
     lat = np.array([r.latency for r in results]) * 1e3
     steps = float(sum(r.particle_steps for r in results))
     kinds = {"ftle": sum(1 for p in plan if p[4]), "recording": sum(1 for p in plan if p[3])}
+
+    def pct(values):
+        v = np.asarray(values, np.float64) * 1e3
+        return {"p50": float(np.percentile(v, 50)), "p99": float(np.percentile(v, 99))} \
+            if len(v) else None
+
+    # Kind of each result by its id (ids are handed out in submission order).
+    kind_of = {}
+    for i, (_, _, _, record, ftle) in enumerate(plan):
+        kind_of[i + 1] = "ftle" if ftle else "recording" if record else "end_positions"
+    by_kind = {}
+    for k in ("end_positions", "recording", "ftle"):
+        rs = [r for r in results if kind_of.get(r.id) == k]
+        by_kind[k] = {"latency_ms": pct([r.latency for r in rs]),
+                      "queue_wait_ms": pct([r.admitted - r.queued for r in rs]),
+                      "service_ms": pct([r.finished - r.admitted for r in rs])}
     return {"requests": len(plan), "completed": len(results), "rate_per_s": rate,
             "seconds_of_arrivals": a.serve_seconds, "wall_seconds": wall,
             "latency_ms": {"p50": float(np.percentile(lat, 50)),
                            "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
+            "queue_wait_ms": pct([r.admitted - r.queued for r in results]),
+            "by_kind": by_kind,
             "particle_steps_per_s": steps / wall, "ticks": int(stats["ticks"]),
             "launches": int(stats["launches"]), "busy_seconds": float(stats["busy_seconds"]),
             "mix": kinds}

@@ -12,7 +12,9 @@
 // (field, integrator, step, recording) group over every in-flight particle of
 // the group's requests, with a step budget, so requests that arrive while
 // others run join at the next tick and share the launches. A request whose
-// particles have all finished is emitted (curve, FTLE) and returned.
+// particles have all finished leaves the ticks at once; a second thread with
+// its own stream copies its results out, emits its curve and FTLE and returns
+// it, while the worker's ticks go on.
 #include <cub/device/device_scan.cuh>
 
 #include <chrono>
@@ -133,8 +135,12 @@ struct dpa_server {
   std::vector<active_request> active;
   std::map<uint64_t, std::unique_ptr<response_storage>> done, handed_out;
   std::deque<uint64_t> done_order;
-  std::thread worker;
+  std::thread worker, finisher;
+  cudaStream_t finish_stream = nullptr;
+  std::deque<active_request> finishing;  // handed from the worker to the finisher
+  std::condition_variable finish_wake;
   bool stopping = false;
+  bool worker_done = false;
   std::string failure;
   uint64_t next_id = 1;
   dpa_server_stats stats{};
@@ -142,7 +148,8 @@ struct dpa_server {
 
   double now() const { return std::chrono::duration<double>(clock_type::now() - start).count(); }
   void run();
-  bool tick();
+  void run_finisher();
+  bool tick(uint64_t steps);
   void select(std::vector<active_request>& out);
   void upload(const active_request& a);
   void finish(active_request& a, response_storage& out);
@@ -156,6 +163,27 @@ namespace {
     if (e_ != cudaSuccess)                                                 \
       throw std::runtime_error(std::string(#expr) + ": " + cudaGetErrorName(e_)); \
   } while (0)
+
+// Per-particle state of a newly admitted request in slots [first, first + n):
+// remaining (and its initial copy) = iterations, in flight, owned by counter
+// `slot`, at time t0, with curve staging at raw_first + i (iterations + 2);
+// the request's in-flight counter = n.
+__global__ void serve_init_kernel(uint64_t first, uint64_t n, uint64_t iterations, float t0,
+                                  uint32_t slot, bool record, uint64_t raw_first,
+                                  uint64_t* remaining, uint64_t* remaining_initial,
+                                  uint8_t* termination, uint32_t* request_of, float* times,
+                                  uint64_t* raw_offsets, unsigned int* in_flight) {
+  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i == 0) in_flight[slot] = unsigned(n);
+  if (i >= n) return;
+  const uint64_t k = first + i;
+  remaining[k] = iterations;
+  remaining_initial[k] = iterations;
+  termination[k] = DPA_TERMINATION_IN_FLIGHT;
+  request_of[k] = slot;
+  times[k] = t0;
+  if (record) raw_offsets[k] = raw_first + i * (iterations + 2);
+}
 
 // Requests advance in step budgets of steps_per_tick, so a particle resumes
 // in a later tick: integrators that carry a derivative from one step to the
@@ -195,46 +223,27 @@ void dpa_server::select(std::vector<active_request>& out) {
   }
 }
 
-// Uploads an admitted request's seeds and resumable state (every particle in
-// flight); worker thread, without the mutex.
+// Starts an admitted request on the device: its seeds are copied in and an
+// init kernel sets its per-particle state (every particle in flight) and its
+// in-flight counter; worker thread, without the mutex. Stream order puts this
+// before the tick that first advances the request.
 void dpa_server::upload(const active_request& a) {
   const dpa_request& q = a.p.request;
   const uint64_t n = q.count, first = a.first;
-  const unsigned int count32 = unsigned(n);
-  SERVER_TRY(cudaMemcpyAsync(in_flight.as<unsigned int>() + a.slot, &count32, 4,
-                             cudaMemcpyHostToDevice, stream));
-  if (n) {
+  if (n)
     SERVER_TRY(cudaMemcpyAsync(positions.as<float>() + 3 * first, a.p.positions.data(), n * 12,
                                cudaMemcpyHostToDevice, stream));
-    std::vector<uint64_t> rem(n, q.iterations), raw_off;
-    std::vector<uint32_t> owner(n, a.slot);
-    std::vector<float> start(n, q.start_time);
-    SERVER_TRY(cudaMemcpyAsync(times.as<float>() + first, start.data(), n * 4,
-                               cudaMemcpyHostToDevice, stream));
-    SERVER_TRY(cudaMemcpyAsync(remaining.as<uint64_t>() + first, rem.data(), n * 8,
-                               cudaMemcpyHostToDevice, stream));
-    SERVER_TRY(cudaMemcpyAsync(remaining_initial.as<uint64_t>() + first, rem.data(), n * 8,
-                               cudaMemcpyHostToDevice, stream));
-    SERVER_TRY(cudaMemsetAsync(termination.as<uint8_t>() + first, DPA_TERMINATION_IN_FLIGHT, n,
-                               stream));
-    SERVER_TRY(cudaMemcpyAsync(request_of.as<uint32_t>() + first, owner.data(), n * 4,
-                               cudaMemcpyHostToDevice, stream));
-    if (q.record) {
-      raw_off.resize(n);
-      for (uint64_t i = 0; i < n; ++i) raw_off[i] = a.raw_first + i * (q.iterations + 2);
-      SERVER_TRY(cudaMemcpyAsync(raw_offsets.as<uint64_t>() + first, raw_off.data(), n * 8,
-                                 cudaMemcpyHostToDevice, stream));
-    }
-    // The host vectors above die at the end of this scope: wait for them.
-    SERVER_TRY(cudaStreamSynchronize(stream));
-  } else {
-    SERVER_TRY(cudaStreamSynchronize(stream));
-  }
+  serve_init_kernel<<<unsigned(std::max<uint64_t>((n + 255) / 256, 1)), 256, 0, stream>>>(
+      first, n, q.iterations, q.start_time, a.slot, q.record != 0, a.raw_first,
+      remaining.as<uint64_t>(), remaining_initial.as<uint64_t>(), termination.as<uint8_t>(),
+      request_of.as<uint32_t>(), times.as<float>(), raw_offsets.as<uint64_t>(),
+      in_flight.as<unsigned int>());
+  SERVER_TRY(cudaGetLastError());
 }
 
 // One tick: a step-budgeted launch per group of requests that can share one.
 // Returns false when nothing was in flight.
-bool dpa_server::tick() {
+bool dpa_server::tick(uint64_t steps) {
   using key_type = std::tuple<int32_t, int32_t, float, int32_t>;  // field, integrator, step, record
   std::map<key_type, std::vector<const active_request*>> groups;
   for (const active_request& a : active) {
@@ -243,14 +252,20 @@ bool dpa_server::tick() {
     groups[{q.field, q.integrator, q.step_size, q.record ? 1 : 0}].push_back(&a);
   }
   if (groups.empty()) return false;
+  // Every group's ranges get their own part of the pinned buffer, so no copy
+  // has to finish before the next group's ranges are written.
+  uint64_t all_ranges = 0;
+  for (auto& g : groups) all_ranges += g.second.size();
+  SERVER_TRY(host_ranges.reserve(all_ranges * 16));
+  uint64_t range_base = 0;
   for (auto& [key, members] : groups) {
     const auto [field_id, integrator, step_size, record] = key;
     const dpa_field* field = fields[size_t(field_id)];
     const uint32_t ranges = uint32_t(members.size());
-    SERVER_TRY(host_ranges.reserve(uint64_t(ranges) * 16));
     SERVER_TRY(starts.reserve(uint64_t(ranges) * 8));
     SERVER_TRY(firsts.reserve(uint64_t(ranges) * 8));
-    uint64_t* h = host_ranges.as<uint64_t>();
+    uint64_t* h = host_ranges.as<uint64_t>() + 2 * range_base;
+    range_base += ranges;
     uint64_t total = 0;
     for (uint32_t r = 0; r < ranges; ++r) {
       h[r] = members[r]->first;
@@ -272,7 +287,7 @@ bool dpa_server::tick() {
     a.remaining = remaining.as<uint64_t>();
     a.termination = termination.as<uint8_t>();
     a.coefficients = dpa::make_step_coefficients(integrator, step_size);
-    a.max_steps = options.steps_per_tick ? options.steps_per_tick : 64;
+    a.max_steps = steps;
     a.claim = ctx->tuning.claim;
     a.work_counter = work_counter.as<unsigned long long>();
     a.resume_only = true;
@@ -288,13 +303,14 @@ bool dpa_server::tick() {
     }
     SERVER_TRY(dpa::launch_advect(field->view, a, integrator, record != 0, stream));
     stats.launches += 1;
-    // (The host ranges are rewritten by the next group: wait for this copy.)
-    SERVER_TRY(cudaStreamSynchronize(stream));
   }
   stats.ticks += 1;
   return true;
 }
 
+// A request whose particles have all finished: copies its end states out,
+// emits its curve and FTLE; finisher thread, on its own stream, without the
+// mutex. The worker no longer touches the request's arena ranges.
 void dpa_server::finish(active_request& a, response_storage& out) {
   const dpa_request& q = a.p.request;
   const uint64_t n = q.count, first = a.first;
@@ -304,13 +320,13 @@ void dpa_server::finish(active_request& a, response_storage& out) {
   out.termination.resize(n);
   if (n) {
     SERVER_TRY(cudaMemcpyAsync(out.positions.data(), positions.as<float>() + 3 * first, n * 12,
-                               cudaMemcpyDeviceToHost, stream));
+                               cudaMemcpyDeviceToHost, finish_stream));
     SERVER_TRY(cudaMemcpyAsync(out.times.data(), times.as<float>() + first, n * 4,
-                               cudaMemcpyDeviceToHost, stream));
+                               cudaMemcpyDeviceToHost, finish_stream));
     SERVER_TRY(cudaMemcpyAsync(out.remaining.data(), remaining.as<uint64_t>() + first, n * 8,
-                               cudaMemcpyDeviceToHost, stream));
+                               cudaMemcpyDeviceToHost, finish_stream));
     SERVER_TRY(cudaMemcpyAsync(out.termination.data(), termination.as<uint8_t>() + first, n,
-                               cudaMemcpyDeviceToHost, stream));
+                               cudaMemcpyDeviceToHost, finish_stream));
   }
   uint64_t vertex_count = 0, index_count = 0;
   if (q.record && n) {
@@ -321,29 +337,29 @@ void dpa_server::finish(active_request& a, response_storage& out) {
     SERVER_TRY(segment_offsets.reserve(n * 8));
     SERVER_TRY(dpa::launch_raw_counts(remaining_initial.as<uint64_t>() + first,
                                       remaining.as<uint64_t>() + first, n,
-                                      raw_counts.as<uint64_t>(), stream));
+                                      raw_counts.as<uint64_t>(), finish_stream));
     auto scan = [&](const uint32_t* in, uint64_t* out_offsets) {
-      SERVER_TRY(dpa::launch_widen_u32(in, n, wide.as<uint64_t>(), stream));
+      SERVER_TRY(dpa::launch_widen_u32(in, n, wide.as<uint64_t>(), finish_stream));
       size_t temp = 0;
       SERVER_TRY(cub::DeviceScan::ExclusiveSum(nullptr, temp, wide.as<uint64_t>(), out_offsets,
-                                               int64_t(n), stream));
+                                               int64_t(n), finish_stream));
       SERVER_TRY(scan_temp.reserve(temp));
       SERVER_TRY(cub::DeviceScan::ExclusiveSum(scan_temp.ptr, temp, wide.as<uint64_t>(),
-                                               out_offsets, int64_t(n), stream));
+                                               out_offsets, int64_t(n), finish_stream));
     };
     scan(kept_vertices.as<uint32_t>() + first, vertex_offsets.as<uint64_t>());
     scan(kept_segments.as<uint32_t>() + first, segment_offsets.as<uint64_t>());
     uint64_t tail[2];
     uint32_t last[2];
     SERVER_TRY(cudaMemcpyAsync(&tail[0], vertex_offsets.as<uint64_t>() + (n - 1), 8,
-                               cudaMemcpyDeviceToHost, stream));
+                               cudaMemcpyDeviceToHost, finish_stream));
     SERVER_TRY(cudaMemcpyAsync(&tail[1], segment_offsets.as<uint64_t>() + (n - 1), 8,
-                               cudaMemcpyDeviceToHost, stream));
+                               cudaMemcpyDeviceToHost, finish_stream));
     SERVER_TRY(cudaMemcpyAsync(&last[0], kept_vertices.as<uint32_t>() + first + (n - 1), 4,
-                               cudaMemcpyDeviceToHost, stream));
+                               cudaMemcpyDeviceToHost, finish_stream));
     SERVER_TRY(cudaMemcpyAsync(&last[1], kept_segments.as<uint32_t>() + first + (n - 1), 4,
-                               cudaMemcpyDeviceToHost, stream));
-    SERVER_TRY(cudaStreamSynchronize(stream));
+                               cudaMemcpyDeviceToHost, finish_stream));
+    SERVER_TRY(cudaStreamSynchronize(finish_stream));
     vertex_count = tail[0] + last[0];
     index_count = 2 * (tail[1] + last[1]);
     const size_t index_bytes = q.index64 ? 8 : 4;
@@ -362,27 +378,26 @@ void dpa_server::finish(active_request& a, response_storage& out) {
     e.vertices = out_vertices.as<float>();
     e.colors = out_colors.as<float>();
     e.indices = out_indices.ptr;
-    SERVER_TRY(dpa::launch_emit(e, q.index64 != 0, true, stream));
+    SERVER_TRY(dpa::launch_emit(e, q.index64 != 0, true, finish_stream));
     out.vertices.resize(3 * vertex_count);
     out.colors.resize(vertex_count);
     SERVER_TRY(cudaMemcpyAsync(out.vertices.data(), out_vertices.ptr, vertex_count * 12,
-                               cudaMemcpyDeviceToHost, stream));
+                               cudaMemcpyDeviceToHost, finish_stream));
     SERVER_TRY(cudaMemcpyAsync(out.colors.data(), out_colors.ptr, vertex_count * 4,
-                               cudaMemcpyDeviceToHost, stream));
+                               cudaMemcpyDeviceToHost, finish_stream));
     if (q.index64) {
       out.indices64.resize(index_count);
       SERVER_TRY(cudaMemcpyAsync(out.indices64.data(), out_indices.ptr, index_count * 8,
-                                 cudaMemcpyDeviceToHost, stream));
+                                 cudaMemcpyDeviceToHost, finish_stream));
     } else {
       out.indices32.resize(index_count);
       SERVER_TRY(cudaMemcpyAsync(out.indices32.data(), out_indices.ptr, index_count * 4,
-                                 cudaMemcpyDeviceToHost, stream));
+                                 cudaMemcpyDeviceToHost, finish_stream));
     }
   }
-  SERVER_TRY(cudaStreamSynchronize(stream));
+  SERVER_TRY(cudaStreamSynchronize(finish_stream));
   uint64_t steps = 0;
   for (uint64_t i = 0; i < n; ++i) steps += q.iterations - out.remaining[i];
-  stats.particle_steps += steps;
   dpa_response& r = out.r;
   r.status = DPA_OK;
   if (q.ftle && n) {
@@ -406,7 +421,7 @@ void dpa_server::finish(active_request& a, response_storage& out) {
       SERVER_TRY(ftle_flow.reserve(cells * 12));
       SERVER_TRY(ftle_out.reserve(cells * 4));
       SERVER_TRY(cudaMemcpyAsync(ftle_original.ptr, a.p.positions.data(), n * 12,
-                                 cudaMemcpyHostToDevice, stream));
+                                 cudaMemcpyHostToDevice, finish_stream));
       f.count = n;
       f.original_positions = ftle_original.as<float>();
       f.final_positions = positions.as<float>() + 3 * first;
@@ -415,11 +430,11 @@ void dpa_server::finish(active_request& a, response_storage& out) {
       f.winners = ftle_winners.as<unsigned long long>();
       f.flow = ftle_flow.as<float>();
       f.ftle = ftle_out.as<float>();
-      SERVER_TRY(dpa::launch_ftle(f, stream));
+      SERVER_TRY(dpa::launch_ftle(f, finish_stream));
       out.ftle.resize(cells);
       SERVER_TRY(cudaMemcpyAsync(out.ftle.data(), ftle_out.ptr, cells * 4, cudaMemcpyDeviceToHost,
-                                 stream));
-      SERVER_TRY(cudaStreamSynchronize(stream));
+                                 finish_stream));
+      SERVER_TRY(cudaStreamSynchronize(finish_stream));
     }
   }
   r.id = a.p.id;
@@ -447,9 +462,12 @@ void dpa_server::run() {
     SERVER_TRY(cudaSetDevice(ctx->device));
     while (true) {
       std::vector<active_request> admitted;
+      bool waiting = false;
       {
         std::unique_lock<std::mutex> lock(mutex);
+        if (!failure.empty()) break;  // the finisher failed
         select(admitted);
+        waiting = !queue.empty();
         if (active.empty() && admitted.empty()) {
           if (stopping && queue.empty()) break;
           wake.wait_for(lock, std::chrono::milliseconds(2));
@@ -463,38 +481,64 @@ void dpa_server::run() {
         stats.admitted += admitted.size();
       }
       const auto t0 = clock_type::now();
-      tick();
+      // While no request waits for admission, ticks run four times as many
+      // steps: fewer launches and syncs per step for the same latency to the
+      // next arrival's admission, which only a waiting request could use.
+      const uint64_t base = options.steps_per_tick ? options.steps_per_tick : 64;
+      tick(waiting ? base : 4 * base);
       // Which requests have no particle in flight any more?
       SERVER_TRY(host_in_flight.reserve(4 * uint64_t(options.max_requests)));
       SERVER_TRY(cudaMemcpyAsync(host_in_flight.ptr, in_flight.ptr, 4 * uint64_t(options.max_requests),
                                  cudaMemcpyDeviceToHost, stream));
       SERVER_TRY(cudaStreamSynchronize(stream));
       const unsigned int* left = host_in_flight.as<unsigned int>();
-      std::vector<std::unique_ptr<response_storage>> finished;
-      std::vector<size_t> finished_at;
-      for (size_t i = 0; i < active.size(); ++i) {
-        if (left[active[i].slot] != 0) continue;
-        auto out = std::make_unique<response_storage>();
-        finish(active[i], *out);
-        finished.push_back(std::move(out));
-        finished_at.push_back(i);
-      }
       stats.busy_seconds += std::chrono::duration<double>(clock_type::now() - t0).count();
       std::lock_guard<std::mutex> lock(mutex);
-      for (size_t j = finished_at.size(); j-- > 0;) {
-        active_request& a = active[finished_at[j]];
-        slots.release(a.first, a.p.request.count);
-        vertices.release(a.raw_first, a.raw_count);
-        free_counters.push_back(a.slot);
-        active.erase(active.begin() + long(finished_at[j]));
+      bool handed = false;
+      for (size_t i = active.size(); i-- > 0;) {
+        if (left[active[i].slot] != 0) continue;
+        finishing.push_back(std::move(active[i]));
+        active.erase(active.begin() + long(i));
+        handed = true;
       }
-      for (auto& out : finished) {
-        const uint64_t id = out->r.id;
-        done_order.push_back(id);
-        done[id] = std::move(out);
-        stats.completed += 1;
+      if (handed) finish_wake.notify_one();
+    }
+  } catch (const std::exception& e) {
+    std::lock_guard<std::mutex> lock(mutex);
+    failure = e.what();
+    stopping = true;
+    done_signal.notify_all();
+  }
+  std::lock_guard<std::mutex> lock(mutex);
+  worker_done = true;
+  finish_wake.notify_all();
+}
+
+void dpa_server::run_finisher() {
+  try {
+    SERVER_TRY(cudaSetDevice(ctx->device));
+    while (true) {
+      active_request a;
+      {
+        std::unique_lock<std::mutex> lock(mutex);
+        finish_wake.wait(lock, [&] { return !finishing.empty() || worker_done; });
+        if (finishing.empty()) break;
+        a = std::move(finishing.front());
+        finishing.pop_front();
       }
-      if (!finished.empty()) done_signal.notify_all();
+      auto out = std::make_unique<response_storage>();
+      finish(a, *out);
+      std::lock_guard<std::mutex> lock(mutex);
+      slots.release(a.first, a.p.request.count);
+      vertices.release(a.raw_first, a.raw_count);
+      free_counters.push_back(a.slot);
+      stats.particle_steps += out->r.particle_steps;
+      stats.completed += 1;
+      const uint64_t id = out->r.id;
+      done_order.push_back(id);
+      done[id] = std::move(out);
+      done_signal.notify_all();
+      wake.notify_one();  // the worker may admit into the freed room
     }
   } catch (const std::exception& e) {
     std::lock_guard<std::mutex> lock(mutex);
@@ -522,6 +566,11 @@ int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_s
       ctx->error = "server: cannot create a stream";
       return DPA_ERROR_CUDA;
     }
+    if (cudaStreamCreateWithFlags(&s->finish_stream, cudaStreamNonBlocking) != cudaSuccess) {
+      cudaStreamDestroy(s->stream);
+      ctx->error = "server: cannot create a stream";
+      return DPA_ERROR_CUDA;
+    }
     const uint64_t p = options->particle_capacity, v = options->vertex_capacity;
     cudaError_t e = cudaSuccess;
     DeviceBuffer* per_slot[] = {&s->positions, &s->times, &s->remaining, &s->remaining_initial,
@@ -537,6 +586,7 @@ int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_s
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     if (e != cudaSuccess) {
       cudaStreamDestroy(s->stream);
+      cudaStreamDestroy(s->finish_stream);
       ctx->error = std::string("server: device arenas: ") + cudaGetErrorName(e);
       return e == cudaErrorMemoryAllocation ? DPA_ERROR_OUT_OF_MEMORY : DPA_ERROR_CUDA;
     }
@@ -545,6 +595,7 @@ int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_s
     for (uint32_t i = options->max_requests; i-- > 0;) s->free_counters.push_back(i);
     dpa_server* raw_ptr = s.get();
     s->worker = std::thread([raw_ptr] { raw_ptr->run(); });
+    s->finisher = std::thread([raw_ptr] { raw_ptr->run_finisher(); });
     *out = s.release();
     return DPA_OK;
   } catch (const std::exception& e) {
@@ -639,9 +690,12 @@ int dpa_server_destroy(dpa_server* s) {
   }
   s->wake.notify_all();
   if (s->worker.joinable()) s->worker.join();
+  if (s->finisher.joinable()) s->finisher.join();
   cudaSetDevice(s->ctx->device);
   cudaStreamSynchronize(s->stream);
+  cudaStreamSynchronize(s->finish_stream);
   cudaStreamDestroy(s->stream);
+  cudaStreamDestroy(s->finish_stream);
   delete s;
   return DPA_OK;
 }

@@ -291,12 +291,16 @@ int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_adve
  * ticks of steps_per_tick steps: one persistent launch per group of requests
  * sharing a field, integrator, step size and recording switch. Requests that
  * arrive while others run join at the next tick. A worker thread owns the
- * device work; submit, poll and stats may be called from any thread. The
- * context is used for its device and its fields only. */
+ * ticks; a second thread, on its own stream, copies out, emits and returns
+ * the requests that have finished while the ticks go on. submit, poll and
+ * stats may be called from any thread. The context is used for its device
+ * and its fields only. */
 typedef struct dpa_server_options {
   uint64_t particle_capacity;  /* particle slots of the arena */
   uint64_t vertex_capacity;    /* curve-staging vertices of the arena (12 bytes each) */
-  uint32_t steps_per_tick;     /* step budget of each tick (0: 64) */
+  uint32_t steps_per_tick;     /* step budget of a tick while requests wait for
+                                  admission (0: 64); four times as many while
+                                  none waits */
   uint32_t max_requests;       /* requests admitted at once */
 } dpa_server_options;
 
