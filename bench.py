@@ -369,25 +369,37 @@ def batched_run(a, ctx, stream, sets=64):
 
 
 def serving_run(a, ctx, rate=200.0):
-    """Poisson arrivals (seed 4) at `rate` requests/s for serve_seconds on a
-    resident 256^3 curl-noise field. Request mix: 10 % FTLE on a 64^3
-    lattice; 50 % recording, seeds log-uniform in [1e2, 2e3] (the returned
-    curves must fit host memory and the link); 40 % end positions, seeds
-    log-uniform in [1e2, 1e6]; iterations uniform in [100, 5000]. Seeds are
-    windows of a pre-drawn pool so that submitting keeps pace with the
-    arrivals. Latency is submit to result; throughput counts particle-steps
-    over the wall time of the run."""
+    """The serving configuration: resident 256^3 and 512^3 curl-noise fields
+    (sigma 4 / seed 1 and sigma 8 / seed 3) and the double gyre on
+    128 x 64 x 64 with 32 time slices; Poisson arrivals (seed 4) at `rate`
+    requests/s for serve_seconds. Request mix: 30 % pathlines through the
+    gyre (start times uniform in [0, 5], step 0.002); 10 % FTLE on a 64^3
+    lattice of the 256^3 field; the rest on either curl-noise field, half of
+    them recording curves. Seeds are log-uniform in [1e2, 1e6], except for
+    recording requests, whose seeds are log-uniform in [1e2, 2e3] so that the
+    returned curves fit host memory and the link; iterations uniform in
+    [100, 5000]. Seeds are windows of pre-drawn pools so that submitting keeps
+    pace with the arrivals. Latency is submit to result; throughput counts
+    particle-steps over the wall time of the run."""
     import threading as th
     from dpa_b200 import fields, seeds
     from dpa_b200.serve import Server
     grid = fields.curl_noise(256, 4.0, 1, device="cuda")
-    field = ctx.field(grid, "f32")
+    big = fields.curl_noise(512, 8.0, 3, device="cuda")
+    gyre = fields.double_gyre()
+    resident = [ctx.field(grid, "f32"), ctx.field(big, "f32"), ctx.field(gyre, "f32")]
     rng = np.random.default_rng(4)
+    pools = []
+    for g, hi in ((grid, 255.0), (big, 511.0)):
+        offset, size = seeds.seed_box(g)
+        pools.append(seeds.generate_random(offset, size, 2_000_000, 0,
+                                           aabb=([0.0] * 3, [hi] * 3), seed=4).position)
+    gyre_hi = gyre.offset + gyre.spacing * (np.array(gyre.shape) - 1)
+    gyre_pool = (gyre.offset + np.random.default_rng(5).random((2_000_000, 3)) *
+                 (gyre_hi - gyre.offset) * 0.999).astype(np.float32)
     offset, size = seeds.seed_box(grid)
-    pool = seeds.generate_random(offset, size, 2_000_000, 0, aabb=([0.0] * 3, [255.0] * 3),
-                                 seed=4).position
     lattice = seeds.generate(offset, size, grid.spacing * np.float32(4), 0).position
-    plan = []
+    plan = []  # (time, field index, seeds, iterations, record, ftle, start time, step)
     t = 0.0
     while True:
         t += rng.exponential(1.0 / rate)
@@ -396,17 +408,25 @@ def serving_run(a, ctx, rate=200.0):
         kind = rng.random()
         iters = int(rng.integers(100, 5001))
         if kind < 0.1:
-            plan.append((t, lattice, iters, False, True))
+            plan.append((t, 0, lattice, iters, False, True, 0.0, a.step_size))
             continue
-        record = kind < 0.6
+        if kind < 0.4:
+            count = int(np.exp(rng.uniform(np.log(1e2), np.log(1e6))))
+            start = int(rng.integers(0, len(gyre_pool) - count))
+            plan.append((t, 2, gyre_pool[start:start + count], iters, False, False,
+                         float(rng.uniform(0.0, 5.0)), 0.002))
+            continue
+        record = kind < 0.7
         hi = 2e3 if record else 1e6
         count = int(np.exp(rng.uniform(np.log(1e2), np.log(hi))))
-        start = int(rng.integers(0, len(pool) - count))
-        plan.append((t, pool[start:start + count], iters, record, False))
+        which = int(rng.integers(0, 2))
+        start = int(rng.integers(0, len(pools[which]) - count))
+        plan.append((t, which, pools[which][start:start + count], iters, record, False, 0.0,
+                     a.step_size))
     results = []
     with Server(ctx, particle_capacity=12_000_000, vertex_capacity=600_000_000,
                 steps_per_tick=64, max_requests=1024) as server:
-        fid = server.add_field(field)
+        fids = [server.add_field(f) for f in resident]
         done = th.Event()
 
         def collect():
@@ -420,20 +440,23 @@ def serving_run(a, ctx, rate=200.0):
         poller = th.Thread(target=collect, daemon=True)
         poller.start()
         t0 = time.perf_counter()
-        for when, pos, iters, record, ftle in plan:
+        for when, which, pos, iters, record, ftle, start_time, step in plan:
             delay = when - (time.perf_counter() - t0)
             if delay > 0:
                 time.sleep(delay)
-            server.submit(fid, pos, iters, a.integrator, a.step_size, record=record, ftle=ftle,
-                          seed_stride=(4.0, 4.0, 4.0))
+            server.submit(fids[which], pos, iters, a.integrator, step, record=record, ftle=ftle,
+                          seed_stride=(4.0, 4.0, 4.0), start_time=start_time)
         done.set()
         poller.join(timeout=600)
         wall = time.perf_counter() - t0
         stats = server.stats()
-    field.close()
+    for f in resident:
+        f.close()
     lat = np.array([r.latency for r in results]) * 1e3
     steps = float(sum(r.particle_steps for r in results))
-    kinds = {"ftle": sum(1 for p in plan if p[4]), "recording": sum(1 for p in plan if p[3])}
+    kinds = {"ftle": sum(1 for p in plan if p[5]), "recording": sum(1 for p in plan if p[4]),
+             "pathlines": sum(1 for p in plan if p[1] == 2),
+             "on_512": sum(1 for p in plan if p[1] == 1)}
 
     def pct(values):
         v = np.asarray(values, np.float64) * 1e3
@@ -442,10 +465,11 @@ def serving_run(a, ctx, rate=200.0):
 
     # Kind of each result by its id (ids are handed out in submission order).
     kind_of = {}
-    for i, (_, _, _, record, ftle) in enumerate(plan):
-        kind_of[i + 1] = "ftle" if ftle else "recording" if record else "end_positions"
+    for i, (_, which, _, _, record, ftle, _, _) in enumerate(plan):
+        kind_of[i + 1] = ("ftle" if ftle else "pathlines" if which == 2 else
+                          "recording" if record else "end_positions")
     by_kind = {}
-    for k in ("end_positions", "recording", "ftle"):
+    for k in ("end_positions", "recording", "pathlines", "ftle"):
         rs = [r for r in results if kind_of.get(r.id) == k]
         by_kind[k] = {"latency_ms": pct([r.latency for r in rs]),
                       "queue_wait_ms": pct([r.admitted - r.queued for r in rs]),

@@ -43,7 +43,8 @@ struct CurveCounter {
 // one of the warp's particles stops, with one vote per step and a 32-bit step
 // counter per stretch (a stretch ends at 2^32 - 1 steps at the latest).
 template <int kIntegrator, int kStorage, bool kPow2, bool kRecord, bool kUnsteady>
-__global__ void __launch_bounds__(kAdvectBlock, kAdvectMinBlocks)
+__global__ void __launch_bounds__(kAdvectBlock,
+                                  kUnsteady ? kAdvectUnsteadyMinBlocks : kAdvectMinBlocks)
 advect_kernel(const FieldView f, const AdvectArgs a) {
   using Sampler = std::conditional_t<kUnsteady, TimeSampler<kStorage, kPow2>,
                                      CellSampler<kStorage, kPow2>>;

@@ -10,6 +10,12 @@ constexpr int kAdvectBlock = 256;
 #define DPA_ADVECT_MIN_BLOCKS 4
 #endif
 constexpr int kAdvectMinBlocks = DPA_ADVECT_MIN_BLOCKS;
+// Time-varying fields: the corner cache holds two slices, so fewer, larger
+// threads (up to 128 registers) per SM.
+#ifndef DPA_ADVECT_UNSTEADY_MIN_BLOCKS
+#define DPA_ADVECT_UNSTEADY_MIN_BLOCKS 2
+#endif
+constexpr int kAdvectUnsteadyMinBlocks = DPA_ADVECT_UNSTEADY_MIN_BLOCKS;
 
 struct AdvectArgs {
   uint64_t count;

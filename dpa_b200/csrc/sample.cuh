@@ -299,11 +299,17 @@ __device__ __forceinline__ bool locate_time(const FieldView& f, float t, int64_t
 }
 
 // Sampler of a time-varying field: the trilinear samples of the two slices
-// around t at p, blended as (1 - w) * a + w * b per component. No corner
-// cache: the two slices' corners would not fit the register budget, and one
-// time window of a field is small enough to stay in L2.
+// around t at p, blended as (1 - w) * a + w * b per component. It caches the
+// corners of both slices for the current cell and slice pair: a pathline
+// usually stays in one cell for many steps and in one slice pair for many
+// more, and the sampled values do not depend on whether the corners came
+// from the cache or from memory.
 template <int kStorage, bool kPow2>
 struct TimeSampler {
+  CornersOf<kStorage> lo, hi;  // slices s and s + 1
+  int cached[3] = {-1, -1, -1};
+  int64_t cached_slice = -1;
+
   __device__ __forceinline__ bool sample(const FieldView& f, const Position& p, float t,
                                          float2& v01, float& v2) {
     int cell[3];
@@ -312,20 +318,29 @@ struct TimeSampler {
     int64_t slice = 0;
     float wt = 0.0f;
     if (!locate_time(f, t, slice, wt)) return false;
-    CornersOf<kStorage> c;
+    if (cell[0] != cached[0] || cell[1] != cached[1] || cell[2] != cached[2] ||
+        slice != cached_slice) {
+      gather<kStorage>(f, cell, lo, slice);
+      gather<kStorage>(f, cell, hi, slice + f.slice_stride);
+      cached[0] = cell[0];
+      cached[1] = cell[1];
+      cached[2] = cell[2];
+      cached_slice = slice;
+    }
     float2 a01, b01;
     float a2, b2;
-    gather<kStorage>(f, cell, c, slice);
-    trilinear(c, w, a01, a2);
-    gather<kStorage>(f, cell, c, slice + f.slice_stride);
-    trilinear(c, w, b01, b2);
+    trilinear(lo, w, a01, a2);
+    trilinear(hi, w, b01, b2);
     const float u = __fsub_rn(1.0f, wt);
     v01 = add2(mul2_scalar(splat(u), a01), mul2_scalar(splat(wt), b01));
     v2 = __fadd_rn(__fmul_rn(u, a2), __fmul_rn(wt, b2));
     return true;
   }
 
-  __device__ __forceinline__ void reset() {}
+  __device__ __forceinline__ void reset() {
+    cached[0] = cached[1] = cached[2] = -1;
+    cached_slice = -1;
+  }
 };
 
 __device__ __forceinline__ bool is_zero(float2 v01, float v2) {
