@@ -362,16 +362,38 @@ def batched_run(a, ctx, stream, sets=64):
         out[storage] = {"ms_per_batch": ms, "particle_steps": steps_total,
                         "particle_steps_per_s": steps_total / (ms / 1e3),
                         "field_device_bytes": field.device_bytes}
+        if storage == "f32":
+            # The plain FP32 path on the same particles: one dpa_advect_device
+            # call over all of them, default launch parameters.
+            plain = []
+            for i in range(3):
+                pos.copy_(p0)
+                rem.copy_(r0)
+                start = torch.cuda.Event(enable_timing=True)
+                end = torch.cuda.Event(enable_timing=True)
+                start.record(stream)
+                ctx.check(lib.dpa_advect_device(ctx.handle, field.handle, C.byref(opts), total,
+                                                C.c_void_p(pos.data_ptr()),
+                                                C.c_void_p(rem.data_ptr()),
+                                                C.c_void_p(term.data_ptr()),
+                                                C.c_void_p(stream.cuda_stream)))
+                end.record(stream)
+                end.synchronize()
+                if i > 0:
+                    plain.append(start.elapsed_time(end))
+            out["plain_f32_ms"] = statistics.mean(plain)
         field.close()
+    out["f16_batched_vs_plain_f32"] = out["plain_f32_ms"] / out["f16"]["ms_per_batch"]
     del p0, r0, pos, rem, term
     torch.cuda.empty_cache()
     return out
 
 
-def serving_run(a, ctx, rate=200.0):
+def serving_run(a, ctx, rate=200.0, storage="f16"):
     """The serving configuration: resident 256^3 and 512^3 curl-noise fields
     (sigma 4 / seed 1 and sigma 8 / seed 3) and the double gyre on
-    128 x 64 x 64 with 32 time slices; Poisson arrivals (seed 4) at `rate`
+    128 x 64 x 64 with 32 time slices, stored in `storage` (the FP16 served
+    form by default); Poisson arrivals (seed 4) at `rate`
     requests/s for serve_seconds. Request mix: 30 % pathlines through the
     gyre (start times uniform in [0, 5], step 0.002); 10 % FTLE on a 64^3
     lattice of the 256^3 field; the rest on either curl-noise field, half of
@@ -387,7 +409,7 @@ def serving_run(a, ctx, rate=200.0):
     grid = fields.curl_noise(256, 4.0, 1, device="cuda")
     big = fields.curl_noise(512, 8.0, 3, device="cuda")
     gyre = fields.double_gyre()
-    resident = [ctx.field(grid, "f32"), ctx.field(big, "f32"), ctx.field(gyre, "f32")]
+    resident = [ctx.field(grid, storage), ctx.field(big, storage), ctx.field(gyre, storage)]
     rng = np.random.default_rng(4)
     pools = []
     for g, hi in ((grid, 255.0), (big, 511.0)):
@@ -475,6 +497,7 @@ def serving_run(a, ctx, rate=200.0):
                       "queue_wait_ms": pct([r.admitted - r.queued for r in rs]),
                       "service_ms": pct([r.finished - r.admitted for r in rs])}
     return {"requests": len(plan), "completed": len(results), "rate_per_s": rate,
+            "field_storage": storage,
             "seconds_of_arrivals": a.serve_seconds, "wall_seconds": wall,
             "latency_ms": {"p50": float(np.percentile(lat, 50)),
                            "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
@@ -717,6 +740,53 @@ def secondary_inputs(a, device):
     return grid, parts.position, 1000, 0.01
 
 
+def recording_at_scale(ctx, a, n=262144, iterations=2000):
+    """Curve recording at scale: the 256^3 curl-noise field, n seeds x
+    `iterations` steps of 0.25, through dpa_advect_round with a sink that
+    takes each chunk without copying it (the curves -- vertices, colors,
+    indices -- still cross to pinned host memory). uint32 and uint64
+    indices."""
+    import ctypes as C
+    from dpa_b200 import _native as N
+    from dpa_b200 import fields, seeds
+    lib = ctx._lib
+    grid = fields.curl_noise(256, 4.0, 1, device="cuda")
+    field = ctx.field(grid)
+    offset, size = seeds.seed_box(grid)
+    pos = seeds.generate_random(offset, size, n, 0, aabb=([0.0] * 3, [255.0] * 3), seed=1).position
+    totals = {"vertices": 0, "indices": 0}
+
+    @N.CURVE_SINK
+    def sink(user, chunk):
+        totals["vertices"] += chunk.contents.vertex_count
+        totals["indices"] += chunk.contents.index_count
+        return 0
+
+    out = {"workload": f"curl-noise 256^3 F32, {n} seeds x {iterations} steps of 0.25, recording",
+           "sink": "takes each chunk in place (no copy)"}
+    for index64 in (0, 1):
+        opts = N.AdvectOptions(N.INTEGRATORS[a.integrator], 0.25, 1, index64, 1, 1, 0)
+        times = []
+        for _ in range(3):
+            hp, hr = pos.copy(), np.full(n, iterations, np.uint64)
+            ht = np.zeros(n, np.uint8)
+            totals.update(vertices=0, indices=0)
+            t0 = time.perf_counter()
+            ctx.check(lib.dpa_advect_round(ctx.handle, field.handle, C.byref(opts), n,
+                                           hp.ctypes.data_as(C.c_void_p),
+                                           hr.ctypes.data_as(C.c_void_p),
+                                           ht.ctypes.data_as(C.c_void_p), sink, None))
+            times.append(time.perf_counter() - t0)
+        t = min(times)
+        steps = float(np.sum(iterations - hr.astype(np.int64)))
+        gb = (totals["vertices"] * 16 + totals["indices"] * (8 if index64 else 4)) / 1e9
+        out["uint64" if index64 else "uint32"] = {
+            "seconds": t, "particle_steps_per_s": steps / t, "vertices": totals["vertices"],
+            "indices": totals["indices"], "curve_GB": gb, "curve_GB_per_s": gb / t}
+    field.close()
+    return out
+
+
 def run_secondary(a):
     """The FTLE and recording configurations: device-timed steps through the
     device entry points (FTLE) or the host round with its curve (recording),
@@ -905,6 +975,7 @@ def run_secondary(a):
                             "is this end-to-end call"},
         })
         algorithmic = None
+        out["at_scale"] = recording_at_scale(ctx, a)
     launches1 = C.c_uint64()
     ctx.check(lib.dpa_context_launch_count(ctx.handle, C.byref(launches1)))
     out["gpu_launches"] = int(launches1.value - launches0.value)

@@ -98,6 +98,7 @@ struct active_request {
   uint64_t raw_first;    // first staging vertex (recording)
   uint64_t raw_count;
   double admitted;
+  uint64_t first_tick;   // the first tick that advances it
 };
 
 struct response_storage {
@@ -119,9 +120,12 @@ struct dpa_server {
   // Particle arena (per slot) and curve staging arena (per vertex).
   DeviceBuffer positions, times, remaining, remaining_initial, termination, raw_offsets,
       kept_vertices, kept_segments, curve_open, request_of, raw, in_flight;
-  // Per tick.
+  // Per tick. Two ticks may be in flight, so the host-side buffers a tick's
+  // copies read or write come in two halves, one per tick parity.
   DeviceBuffer list, starts, firsts, work_counter;
-  PinnedBuffer host_ranges, host_in_flight;
+  PinnedBuffer host_ranges[2], host_in_flight;
+  cudaStream_t upload_stream = nullptr;  // seed copies, beside the running tick
+  cudaEvent_t seeds_copied = nullptr, readback[2] = {nullptr, nullptr};
   // Emission scratch.
   DeviceBuffer raw_counts, wide, vertex_offsets, segment_offsets, scan_temp, out_vertices,
       out_colors, out_indices;
@@ -149,9 +153,20 @@ struct dpa_server {
   double now() const { return std::chrono::duration<double>(clock_type::now() - start).count(); }
   void run();
   void run_finisher();
-  bool tick(uint64_t steps);
+  void destroy_streams() {
+    for (cudaStream_t st : {stream, finish_stream, upload_stream})
+      if (st) {
+        cudaStreamSynchronize(st);
+        cudaStreamDestroy(st);
+      }
+    for (cudaEvent_t ev : {seeds_copied, readback[0], readback[1]})
+      if (ev) cudaEventDestroy(ev);
+    stream = finish_stream = upload_stream = nullptr;
+    seeds_copied = readback[0] = readback[1] = nullptr;
+  }
+  bool tick(uint64_t steps, int parity);
   void select(std::vector<active_request>& out);
-  void upload(const active_request& a);
+  void upload(std::vector<active_request>& admitted, uint64_t first_tick);
   void finish(active_request& a, response_storage& out);
 };
 
@@ -223,27 +238,38 @@ void dpa_server::select(std::vector<active_request>& out) {
   }
 }
 
-// Starts an admitted request on the device: its seeds are copied in and an
-// init kernel sets its per-particle state (every particle in flight) and its
-// in-flight counter; worker thread, without the mutex. Stream order puts this
-// before the tick that first advances the request.
-void dpa_server::upload(const active_request& a) {
-  const dpa_request& q = a.p.request;
-  const uint64_t n = q.count, first = a.first;
-  if (n)
-    SERVER_TRY(cudaMemcpyAsync(positions.as<float>() + 3 * first, a.p.positions.data(), n * 12,
-                               cudaMemcpyHostToDevice, stream));
-  serve_init_kernel<<<unsigned(std::max<uint64_t>((n + 255) / 256, 1)), 256, 0, stream>>>(
-      first, n, q.iterations, q.start_time, a.slot, q.record != 0, a.raw_first,
-      remaining.as<uint64_t>(), remaining_initial.as<uint64_t>(), termination.as<uint8_t>(),
-      request_of.as<uint32_t>(), times.as<float>(), raw_offsets.as<uint64_t>(),
-      in_flight.as<unsigned int>());
-  SERVER_TRY(cudaGetLastError());
+// Starts admitted requests on the device: their seeds are copied in on the
+// upload stream, beside the running tick (whose particles never share slots
+// with them: a slot is reused only after its request has finished and been
+// returned, and ticks skip finished particles); then, in the ticks' stream
+// order, an init kernel per request sets its per-particle state (every
+// particle in flight) and its in-flight counter. Worker thread, without the
+// mutex.
+void dpa_server::upload(std::vector<active_request>& admitted, uint64_t first_tick) {
+  for (active_request& a : admitted) {
+    a.first_tick = first_tick;
+    const uint64_t n = a.p.request.count;
+    if (n)
+      SERVER_TRY(cudaMemcpyAsync(positions.as<float>() + 3 * a.first, a.p.positions.data(),
+                                 n * 12, cudaMemcpyHostToDevice, upload_stream));
+  }
+  SERVER_TRY(cudaEventRecord(seeds_copied, upload_stream));
+  SERVER_TRY(cudaStreamWaitEvent(stream, seeds_copied, 0));
+  for (const active_request& a : admitted) {
+    const dpa_request& q = a.p.request;
+    const uint64_t n = q.count;
+    serve_init_kernel<<<unsigned(std::max<uint64_t>((n + 255) / 256, 1)), 256, 0, stream>>>(
+        a.first, n, q.iterations, q.start_time, a.slot, q.record != 0, a.raw_first,
+        remaining.as<uint64_t>(), remaining_initial.as<uint64_t>(), termination.as<uint8_t>(),
+        request_of.as<uint32_t>(), times.as<float>(), raw_offsets.as<uint64_t>(),
+        in_flight.as<unsigned int>());
+    SERVER_TRY(cudaGetLastError());
+  }
 }
 
 // One tick: a step-budgeted launch per group of requests that can share one.
 // Returns false when nothing was in flight.
-bool dpa_server::tick(uint64_t steps) {
+bool dpa_server::tick(uint64_t steps, int parity) {
   using key_type = std::tuple<int32_t, int32_t, float, int32_t>;  // field, integrator, step, record
   std::map<key_type, std::vector<const active_request*>> groups;
   for (const active_request& a : active) {
@@ -256,7 +282,8 @@ bool dpa_server::tick(uint64_t steps) {
   // has to finish before the next group's ranges are written.
   uint64_t all_ranges = 0;
   for (auto& g : groups) all_ranges += g.second.size();
-  SERVER_TRY(host_ranges.reserve(all_ranges * 16));
+  PinnedBuffer& host = host_ranges[parity];
+  SERVER_TRY(host.reserve(all_ranges * 16));
   uint64_t range_base = 0;
   for (auto& [key, members] : groups) {
     const auto [field_id, integrator, step_size, record] = key;
@@ -264,7 +291,7 @@ bool dpa_server::tick(uint64_t steps) {
     const uint32_t ranges = uint32_t(members.size());
     SERVER_TRY(starts.reserve(uint64_t(ranges) * 8));
     SERVER_TRY(firsts.reserve(uint64_t(ranges) * 8));
-    uint64_t* h = host_ranges.as<uint64_t>() + 2 * range_base;
+    uint64_t* h = host.as<uint64_t>() + 2 * range_base;
     range_base += ranges;
     uint64_t total = 0;
     for (uint32_t r = 0; r < ranges; ++r) {
@@ -457,9 +484,19 @@ void dpa_server::finish(active_request& a, response_storage& out) {
   r.finished_seconds = now();
 }
 
+// The worker keeps the GPU fed: it launches tick k and only then looks at
+// tick k - 1's in-flight counters, so tick k runs while the host admits,
+// uploads and hands finished requests to the finisher. A request finishing in
+// tick k - 1 may still be in tick k's launch list; tick k skips its finished
+// particles.
 void dpa_server::run() {
   try {
     SERVER_TRY(cudaSetDevice(ctx->device));
+    const uint64_t counters = options.max_requests;
+    SERVER_TRY(host_in_flight.reserve(2 * 4 * counters));
+    uint64_t next_tick = 0;
+    bool pending = false;  // a launched tick whose counters are not read yet
+    uint64_t pending_tick = 0;
     while (true) {
       std::vector<active_request> admitted;
       bool waiting = false;
@@ -468,40 +505,54 @@ void dpa_server::run() {
         if (!failure.empty()) break;  // the finisher failed
         select(admitted);
         waiting = !queue.empty();
-        if (active.empty() && admitted.empty()) {
+        if (active.empty() && admitted.empty() && !pending) {
           if (stopping && queue.empty()) break;
           wake.wait_for(lock, std::chrono::milliseconds(2));
           continue;
         }
       }
-      for (const active_request& a : admitted) upload(a);
-      {
+      const auto t0 = clock_type::now();
+      if (!admitted.empty()) {
+        upload(admitted, next_tick);
         std::lock_guard<std::mutex> lock(mutex);
         for (active_request& a : admitted) active.push_back(std::move(a));
         stats.admitted += admitted.size();
       }
-      const auto t0 = clock_type::now();
-      // While no request waits for admission, ticks run four times as many
-      // steps: fewer launches and syncs per step for the same latency to the
-      // next arrival's admission, which only a waiting request could use.
-      const uint64_t base = options.steps_per_tick ? options.steps_per_tick : 64;
-      tick(waiting ? base : 4 * base);
-      // Which requests have no particle in flight any more?
-      SERVER_TRY(host_in_flight.reserve(4 * uint64_t(options.max_requests)));
-      SERVER_TRY(cudaMemcpyAsync(host_in_flight.ptr, in_flight.ptr, 4 * uint64_t(options.max_requests),
-                                 cudaMemcpyDeviceToHost, stream));
-      SERVER_TRY(cudaStreamSynchronize(stream));
-      const unsigned int* left = host_in_flight.as<unsigned int>();
-      stats.busy_seconds += std::chrono::duration<double>(clock_type::now() - t0).count();
-      std::lock_guard<std::mutex> lock(mutex);
-      bool handed = false;
-      for (size_t i = active.size(); i-- > 0;) {
-        if (left[active[i].slot] != 0) continue;
-        finishing.push_back(std::move(active[i]));
-        active.erase(active.begin() + long(i));
-        handed = true;
+      bool launched = false;
+      const int parity = int(next_tick & 1);
+      if (!active.empty()) {
+        // While no request waits for admission, ticks run four times as many
+        // steps: fewer launches per step for the same latency to the next
+        // arrival's admission, which only a waiting request could use.
+        const uint64_t base = options.steps_per_tick ? options.steps_per_tick : 64;
+        tick(waiting ? base : 4 * base, parity);
+        // Which requests have no particle in flight any more?
+        SERVER_TRY(cudaMemcpyAsync(host_in_flight.as<unsigned int>() + parity * counters,
+                                   in_flight.ptr, 4 * counters, cudaMemcpyDeviceToHost, stream));
+        SERVER_TRY(cudaEventRecord(readback[parity], stream));
+        launched = true;
       }
-      if (handed) finish_wake.notify_one();
+      if (pending) {
+        SERVER_TRY(cudaEventSynchronize(readback[pending_tick & 1]));
+        const unsigned int* left =
+            host_in_flight.as<unsigned int>() + (pending_tick & 1) * counters;
+        std::lock_guard<std::mutex> lock(mutex);
+        bool handed = false;
+        for (size_t i = active.size(); i-- > 0;) {
+          // Requests admitted after that tick have not been counted yet.
+          if (active[i].first_tick > pending_tick || left[active[i].slot] != 0) continue;
+          finishing.push_back(std::move(active[i]));
+          active.erase(active.begin() + long(i));
+          handed = true;
+        }
+        if (handed) finish_wake.notify_one();
+        pending = false;
+      }
+      if (launched) {
+        pending = true;
+        pending_tick = next_tick++;
+      }
+      stats.busy_seconds += std::chrono::duration<double>(clock_type::now() - t0).count();
     }
   } catch (const std::exception& e) {
     std::lock_guard<std::mutex> lock(mutex);
@@ -566,8 +617,12 @@ int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_s
       ctx->error = "server: cannot create a stream";
       return DPA_ERROR_CUDA;
     }
-    if (cudaStreamCreateWithFlags(&s->finish_stream, cudaStreamNonBlocking) != cudaSuccess) {
-      cudaStreamDestroy(s->stream);
+    if (cudaStreamCreateWithFlags(&s->finish_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->upload_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->seeds_copied, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->readback[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->readback[1], cudaEventDisableTiming) != cudaSuccess) {
+      s->destroy_streams();
       ctx->error = "server: cannot create a stream";
       return DPA_ERROR_CUDA;
     }
@@ -585,8 +640,7 @@ int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_s
       e = cudaMemsetAsync(s->in_flight.ptr, 0, 4 * uint64_t(options->max_requests), s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     if (e != cudaSuccess) {
-      cudaStreamDestroy(s->stream);
-      cudaStreamDestroy(s->finish_stream);
+      s->destroy_streams();
       ctx->error = std::string("server: device arenas: ") + cudaGetErrorName(e);
       return e == cudaErrorMemoryAllocation ? DPA_ERROR_OUT_OF_MEMORY : DPA_ERROR_CUDA;
     }
@@ -692,10 +746,7 @@ int dpa_server_destroy(dpa_server* s) {
   if (s->worker.joinable()) s->worker.join();
   if (s->finisher.joinable()) s->finisher.join();
   cudaSetDevice(s->ctx->device);
-  cudaStreamSynchronize(s->stream);
-  cudaStreamSynchronize(s->finish_stream);
-  cudaStreamDestroy(s->stream);
-  cudaStreamDestroy(s->finish_stream);
+  s->destroy_streams();
   delete s;
   return DPA_OK;
 }
