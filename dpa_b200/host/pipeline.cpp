@@ -6,15 +6,19 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <deque>
 #include <filesystem>
 #include <fstream>
 #include <functional>
 #include <iostream>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <sstream>
 #include <stdexcept>
+#include <thread>
 
 #include "dpa_b200.h"
 #include "hdf5.hpp"
@@ -156,6 +160,94 @@ struct round_curve {
   std::vector<uint32_t> indices32;
   std::vector<uint64_t> indices64;
   bool index64 = false;
+};
+
+// Writes each round's curve (integral_curve_saver.cpp:44-79: vertices_i,
+// colors_i, indices_i) on a background thread while the next round advects.
+// At most two finished rounds wait in memory; push() blocks beyond that.
+class round_writer {
+ public:
+  round_writer(h5::writer& out, std::string file, bool index64)
+      : out_(out), file_(std::move(file)), index64_(index64), thread_([this] { run(); }) {}
+  ~round_writer() {
+    if (thread_.joinable()) {
+      {
+        std::lock_guard<std::mutex> lock(mutex_);
+        done_ = true;
+      }
+      wake_.notify_all();
+      thread_.join();
+    }
+  }
+
+  // Hands a round's curve over; returns the milliseconds spent waiting for
+  // room (the writer falling behind the rounds).
+  float push(uint64_t round, round_curve&& curve) {
+    const auto t0 = std::chrono::high_resolution_clock::now();
+    std::unique_lock<std::mutex> lock(mutex_);
+    room_.wait(lock, [&] { return queue_.size() < 2 || failed_; });
+    if (failed_) throw std::runtime_error(error_);
+    queue_.emplace_back(round, std::move(curve));
+    wake_.notify_all();
+    return std::chrono::duration<float, std::milli>(std::chrono::high_resolution_clock::now() - t0)
+        .count();
+  }
+
+  // Waits for every round to be written; returns the XDMF grids.
+  std::string finish() {
+    {
+      std::lock_guard<std::mutex> lock(mutex_);
+      done_ = true;
+    }
+    wake_.notify_all();
+    thread_.join();
+    if (failed_) throw std::runtime_error(error_);
+    return xdmf_;
+  }
+
+ private:
+  void run() {
+    while (true) {
+      std::pair<uint64_t, round_curve> item;
+      {
+        std::unique_lock<std::mutex> lock(mutex_);
+        wake_.wait(lock, [&] { return !queue_.empty() || done_; });
+        if (queue_.empty()) return;
+        item = std::move(queue_.front());
+      }
+      try {
+        const round_curve& c = item.second;
+        const uint64_t v = c.vertices.size() / 3;
+        const uint64_t ni = index64_ ? c.indices64.size() : c.indices32.size();
+        const std::string r = std::to_string(item.first);
+        out_.add_dataset("vertices_" + r, h5::element::f32, {3 * v}, c.vertices.data());
+        out_.add_dataset("colors_" + r, h5::element::f32, {v}, c.colors.data());
+        if (index64_)
+          out_.add_dataset("indices_" + r, h5::element::u64, {ni}, c.indices64.data());
+        else
+          out_.add_dataset("indices_" + r, h5::element::u32, {ni}, c.indices32.data());
+        xdmf_ += xdmf_polyline(file_, item.first, v, ni, index64_);
+      } catch (const std::exception& e) {
+        std::lock_guard<std::mutex> lock(mutex_);
+        failed_ = true;
+        error_ = e.what();
+      }
+      std::lock_guard<std::mutex> lock(mutex_);
+      queue_.pop_front();
+      room_.notify_all();
+      if (failed_) return;
+    }
+  }
+
+  h5::writer& out_;
+  const std::string file_;
+  const bool index64_;
+  std::mutex mutex_;
+  std::condition_variable wake_, room_;
+  std::deque<std::pair<uint64_t, round_curve>> queue_;
+  bool done_ = false, failed_ = false;
+  std::string error_, xdmf_;
+  std::thread thread_;
 };
 
 int collect_chunk(void* user, const dpa_curve_chunk* c) {
@@ -345,9 +437,13 @@ int run(const std::string& config_path) {
     const std::string curve_path =
         std::filesystem::path(args.output_dataset_filepath).replace_extension(".rank_0.h5").string();
     std::unique_ptr<h5::writer> curves;
+    std::unique_ptr<round_writer> writer;
     std::string xdmf_bodies;
-    if (args.particle_advector_record) curves = std::make_unique<h5::writer>(curve_path);
     const std::string curve_file = std::filesystem::path(curve_path).filename().string();
+    if (args.particle_advector_record) {
+      curves = std::make_unique<h5::writer>(curve_path);
+      writer = std::make_unique<round_writer>(*curves, curve_file, index64);
+    }
 
     uint64_t active = total;
     uint64_t rounds = 0;
@@ -374,27 +470,15 @@ int run(const std::string& config_path) {
           });
           rec.record(prefix + ".communication_time", [&]() { complete = active == 0; });
         });
-        if (curves && !curve.vertices.empty()) {
-          const auto t0 = std::chrono::high_resolution_clock::now();
-          const uint64_t v = curve.vertices.size() / 3;
-          const uint64_t ni = index64 ? curve.indices64.size() : curve.indices32.size();
-          const std::string r = std::to_string(rounds);
-          curves->add_dataset("vertices_" + r, h5::element::f32, {3 * v}, curve.vertices.data());
-          curves->add_dataset("colors_" + r, h5::element::f32, {v}, curve.colors.data());
-          if (index64)
-            curves->add_dataset("indices_" + r, h5::element::u64, {ni}, curve.indices64.data());
-          else
-            curves->add_dataset("indices_" + r, h5::element::u32, {ni}, curve.indices32.data());
-          xdmf_bodies += xdmf_polyline(curve_file, rounds, v, ni, index64);
-          io_ms += std::chrono::duration<float, std::milli>(
-                       std::chrono::high_resolution_clock::now() - t0)
-                       .count();
-        }
+        // The round's curve is written in the background while the next
+        // round advects.
+        if (writer && !curve.vertices.empty()) io_ms += writer->push(rounds, std::move(curve));
         ++rounds;
       }
     }
     // total_time covers the round loop as in the reference (pipeline.cpp:98);
-    // this build writes each round's curve between rounds, which is taken out.
+    // the curve writes overlap the rounds, and any wait for the writer is
+    // taken out.
     const float loop_ms = std::chrono::duration<float, std::milli>(
                               std::chrono::high_resolution_clock::now() - loop_start)
                               .count();
@@ -406,6 +490,7 @@ int run(const std::string& config_path) {
     std::cout << "color_generation\n";
     std::cout << "save_integral_curves\n";
     if (curves) {
+      xdmf_bodies = writer->finish();
       curves->close();
       if (!xdmf_bodies.empty()) {
         std::ofstream x(curve_path + ".xdmf");

@@ -125,3 +125,12 @@ def test_seed_generators_agree_across_python_and_host(oracle):
         assert lo <= n <= hi and n == seeds.random_count(lo, hi, seed)
     u = seeds.random_unit(100000, 4)
     assert u.min() >= 0.0 and u.max() < 1.0 and abs(float(u.mean()) - 0.5) < 0.01
+
+
+@pytest.mark.skipif(not Path("/dev/full").exists(), reason="no /dev/full")
+def test_writer_reports_a_short_write():
+    # A device whose every write fails with ENOSPC: the writer must raise,
+    # not leave a silently truncated file behind.
+    data = {"vertices_0": np.arange(3 * 100000, dtype=np.float32)}
+    with pytest.raises(RuntimeError, match="short write|cannot close"):
+        host.write_datasets("/dev/full", data)
