@@ -53,7 +53,8 @@ def parse_args():
                         "curves with uint32 indices")
     p.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
     p.add_argument("--integrator", default="runge_kutta_4")
-    p.add_argument("--n", type=int, default=256)
+    p.add_argument("--grid", dest="n", type=int, default=256,
+                   help="grid points per axis of the throughput workload")
     p.add_argument("--seeds", type=int, default=1 << 20)
     p.add_argument("--iterations", type=int, default=2000)
     p.add_argument("--step-size", type=float, default=0.25)
@@ -145,13 +146,34 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sms)}
 
 
-def make_inputs(a, rank, device):
-    from dpa_b200 import fields, seeds
-    grid = fields.curl_noise(a.n, 4.0, 1, spacing=1.0, device=device)
+def rank_seeds(grid, count, iterations, rank):
+    """The seed set of one replica: `count` uniform seeds in the valid domain
+    of the grid, drawn from stream 1 + rank, so every rank advects its own
+    independent particles through the same (replicated) field."""
+    from dpa_b200 import seeds
     offset, size = seeds.seed_box(grid)
-    box = ([0.0, 0.0, 0.0], [float(a.n - 1)] * 3)
-    parts = seeds.generate_random(offset, size, a.seeds, a.iterations, aabb=box, seed=1 + rank)
-    return grid, parts
+    box = ([0.0, 0.0, 0.0], [float(s - 1) for s in grid.shape])
+    return seeds.generate_random(offset, size, count, iterations, aabb=box, seed=1 + rank)
+
+
+def make_inputs(a, rank, device):
+    from dpa_b200 import fields
+    grid = fields.curl_noise(a.n, 4.0, 1, spacing=1.0, device=device)
+    return grid, rank_seeds(grid, a.seeds, a.iterations, rank)
+
+
+def combine_over_ranks(ms, steps, device):
+    """Whole-job figures of the replicas: the slowest rank's time and the
+    particle-steps of all ranks (max and sum over the process group when there
+    is one). Returns (ms_max, steps_total)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    n = torch.tensor([float(steps)], dtype=torch.float64, device=device)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(n, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(n.item())
 
 
 def cpu_baseline(a, grid, parts, target_seconds, steps_budget=None):
@@ -624,13 +646,8 @@ def run_gpu(a):
     rem_out = rem.cpu().numpy().astype(np.int64)
     steps_taken = float(np.sum(a.iterations - rem_out))
     ms_per_step = total_ms / a.steps
-    t = torch.tensor([ms_per_step], dtype=torch.float64, device="cuda")
-    s = torch.tensor([steps_taken], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(s, op=dist.ReduceOp.SUM)
-    ms_max = float(t.item())
-    value = float(s.item()) / (ms_max / 1e3)
+    ms_max, steps_total = combine_over_ranks(ms_per_step, steps_taken, "cuda")
+    value = steps_total / (ms_max / 1e3)
     gpu_final = pos.cpu().numpy()
 
     # End to end through the host C ABI with pinned host buffers.
@@ -653,12 +670,8 @@ def run_gpu(a):
     e2e_once()
     e2e_times = [e2e_once() for _ in range(e2e_steps)]
     e2e_steps_taken = float(np.sum(a.iterations - host_rem.astype(np.int64)))
-    e2e_t = torch.tensor([statistics.mean(e2e_times)], dtype=torch.float64, device="cuda")
-    e2e_s = torch.tensor([e2e_steps_taken], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-        dist.all_reduce(e2e_s, op=dist.ReduceOp.SUM)
-    e2e_value = float(e2e_s.item()) / float(e2e_t.item())
+    e2e_max, e2e_total = combine_over_ranks(statistics.mean(e2e_times), e2e_steps_taken, "cuda")
+    e2e_value = e2e_total / e2e_max
 
     peak, peak_src = measured_peak_hbm()
     kernel_s = statistics.mean(kernel_ms) / 1e3
@@ -677,7 +690,7 @@ def run_gpu(a):
         "warmup": a.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(a, world),
-        "particle_steps_per_step": float(s.item()),
+        "particle_steps_per_step": steps_total,
         "kernel_ms": statistics.mean(kernel_ms), "order_ms": statistics.mean(order_ms),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
