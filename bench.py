@@ -527,6 +527,7 @@ def serving_run(a, ctx, rate=200.0, storage="f16"):
             "by_kind": by_kind,
             "particle_steps_per_s": steps / wall, "ticks": int(stats["ticks"]),
             "launches": int(stats["launches"]), "busy_seconds": float(stats["busy_seconds"]),
+            "tick_device_seconds": float(stats["tick_device_seconds"]),
             "mix": kinds}
 
 

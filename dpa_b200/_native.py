@@ -138,6 +138,7 @@ class ServerStats(C.Structure):
         ("busy_seconds", C.c_double),
         ("queued", C.c_uint32),
         ("active", C.c_uint32),
+        ("tick_device_seconds", C.c_double),
     ]
 
 

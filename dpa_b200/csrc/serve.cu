@@ -126,6 +126,7 @@ struct dpa_server {
   PinnedBuffer host_ranges[2], host_in_flight;
   cudaStream_t upload_stream = nullptr;  // seed copies, beside the running tick
   cudaEvent_t seeds_copied = nullptr, readback[2] = {nullptr, nullptr};
+  cudaEvent_t tick_start[2] = {nullptr, nullptr};  // device time of each tick
   // Emission scratch.
   DeviceBuffer raw_counts, wide, vertex_offsets, segment_offsets, scan_temp, out_vertices,
       out_colors, out_indices;
@@ -159,10 +160,10 @@ struct dpa_server {
         cudaStreamSynchronize(st);
         cudaStreamDestroy(st);
       }
-    for (cudaEvent_t ev : {seeds_copied, readback[0], readback[1]})
+    for (cudaEvent_t ev : {seeds_copied, readback[0], readback[1], tick_start[0], tick_start[1]})
       if (ev) cudaEventDestroy(ev);
     stream = finish_stream = upload_stream = nullptr;
-    seeds_copied = readback[0] = readback[1] = nullptr;
+    seeds_copied = readback[0] = readback[1] = tick_start[0] = tick_start[1] = nullptr;
   }
   bool tick(uint64_t steps, int parity);
   void select(std::vector<active_request>& out);
@@ -525,6 +526,7 @@ void dpa_server::run() {
         // steps: fewer launches per step for the same latency to the next
         // arrival's admission, which only a waiting request could use.
         const uint64_t base = options.steps_per_tick ? options.steps_per_tick : 64;
+        SERVER_TRY(cudaEventRecord(tick_start[parity], stream));
         tick(waiting ? base : 4 * base, parity);
         // Which requests have no particle in flight any more?
         SERVER_TRY(cudaMemcpyAsync(host_in_flight.as<unsigned int>() + parity * counters,
@@ -536,7 +538,11 @@ void dpa_server::run() {
         SERVER_TRY(cudaEventSynchronize(readback[pending_tick & 1]));
         const unsigned int* left =
             host_in_flight.as<unsigned int>() + (pending_tick & 1) * counters;
+        float tick_ms = 0.0f;
+        SERVER_TRY(cudaEventElapsedTime(&tick_ms, tick_start[pending_tick & 1],
+                                        readback[pending_tick & 1]));
         std::lock_guard<std::mutex> lock(mutex);
+        stats.tick_device_seconds += 1e-3 * double(tick_ms);
         bool handed = false;
         for (size_t i = active.size(); i-- > 0;) {
           // Requests admitted after that tick have not been counted yet.
@@ -620,8 +626,10 @@ int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_s
     if (cudaStreamCreateWithFlags(&s->finish_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&s->upload_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->seeds_copied, cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&s->readback[0], cudaEventDisableTiming) != cudaSuccess ||
-        cudaEventCreateWithFlags(&s->readback[1], cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventCreate(&s->readback[0]) != cudaSuccess ||
+        cudaEventCreate(&s->readback[1]) != cudaSuccess ||
+        cudaEventCreate(&s->tick_start[0]) != cudaSuccess ||
+        cudaEventCreate(&s->tick_start[1]) != cudaSuccess) {
       s->destroy_streams();
       ctx->error = "server: cannot create a stream";
       return DPA_ERROR_CUDA;

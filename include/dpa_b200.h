@@ -351,9 +351,12 @@ typedef struct dpa_server_stats {
   uint64_t ticks;
   uint64_t launches;
   uint64_t particle_steps;
-  double   busy_seconds;
+  double   busy_seconds;         /* worker time spent on ticks (host side) */
   uint32_t queued;
   uint32_t active;
+  double   tick_device_seconds;  /* device time of the ticks (their launches, in
+                                    stream order; overlapping finishing work on
+                                    the finisher's stream is not counted) */
 } dpa_server_stats;
 
 int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_server** out);
