@@ -36,6 +36,8 @@ namespace {
 
 using clock_type = std::chrono::steady_clock;
 
+constexpr size_t kMaxServerFields = 256;
+
 // First-fit allocator of [0, capacity) ranges, coalescing on free.
 class range_allocator {
  public:
@@ -165,7 +167,7 @@ struct dpa_server {
     stream = finish_stream = upload_stream = nullptr;
     seeds_copied = readback[0] = readback[1] = tick_start[0] = tick_start[1] = nullptr;
   }
-  bool tick(uint64_t steps, int parity);
+  uint32_t tick(uint64_t steps, int parity);
   void select(std::vector<active_request>& out);
   void upload(std::vector<active_request>& admitted, uint64_t first_tick);
   void finish(active_request& a, response_storage& out);
@@ -270,7 +272,7 @@ void dpa_server::upload(std::vector<active_request>& admitted, uint64_t first_ti
 
 // One tick: a step-budgeted launch per group of requests that can share one.
 // Returns false when nothing was in flight.
-bool dpa_server::tick(uint64_t steps, int parity) {
+uint32_t dpa_server::tick(uint64_t steps, int parity) {
   using key_type = std::tuple<int32_t, int32_t, float, int32_t>;  // field, integrator, step, record
   std::map<key_type, std::vector<const active_request*>> groups;
   for (const active_request& a : active) {
@@ -278,11 +280,12 @@ bool dpa_server::tick(uint64_t steps, int parity) {
     if (q.count == 0) continue;
     groups[{q.field, q.integrator, q.step_size, q.record ? 1 : 0}].push_back(&a);
   }
-  if (groups.empty()) return false;
+  if (groups.empty()) return 0;
   // Every group's ranges get their own part of the pinned buffer, so no copy
   // has to finish before the next group's ranges are written.
   uint64_t all_ranges = 0;
   for (auto& g : groups) all_ranges += g.second.size();
+  uint32_t launched = 0;
   PinnedBuffer& host = host_ranges[parity];
   SERVER_TRY(host.reserve(all_ranges * 16));
   uint64_t range_base = 0;
@@ -330,10 +333,9 @@ bool dpa_server::tick(uint64_t steps, int parity) {
       a.curve_open = curve_open.as<uint8_t>();
     }
     SERVER_TRY(dpa::launch_advect(field->view, a, integrator, record != 0, stream));
-    stats.launches += 1;
+    ++launched;
   }
-  stats.ticks += 1;
-  return true;
+  return launched;
 }
 
 // A request whose particles have all finished: copies its end states out,
@@ -527,7 +529,12 @@ void dpa_server::run() {
         // arrival's admission, which only a waiting request could use.
         const uint64_t base = options.steps_per_tick ? options.steps_per_tick : 64;
         SERVER_TRY(cudaEventRecord(tick_start[parity], stream));
-        tick(waiting ? base : 4 * base, parity);
+        const uint32_t launches = tick(waiting ? base : 4 * base, parity);
+        {
+          std::lock_guard<std::mutex> lock(mutex);
+          stats.launches += launches;
+          stats.ticks += 1;
+        }
         // Which requests have no particle in flight any more?
         SERVER_TRY(cudaMemcpyAsync(host_in_flight.as<unsigned int>() + parity * counters,
                                    in_flight.ptr, 4 * counters, cudaMemcpyDeviceToHost, stream));
@@ -558,6 +565,7 @@ void dpa_server::run() {
         pending = true;
         pending_tick = next_tick++;
       }
+      std::lock_guard<std::mutex> lock(mutex);
       stats.busy_seconds += std::chrono::duration<double>(clock_type::now() - t0).count();
     }
   } catch (const std::exception& e) {
@@ -652,6 +660,7 @@ int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_s
       ctx->error = std::string("server: device arenas: ") + cudaGetErrorName(e);
       return e == cudaErrorMemoryAllocation ? DPA_ERROR_OUT_OF_MEMORY : DPA_ERROR_CUDA;
     }
+    s->fields.reserve(kMaxServerFields);
     s->slots.reset(p);
     s->vertices.reset(v);
     for (uint32_t i = options->max_requests; i-- > 0;) s->free_counters.push_back(i);
@@ -669,6 +678,12 @@ int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_s
 int dpa_server_add_field(dpa_server* s, const dpa_field* field, int32_t* id) {
   if (!s || !field || !id || field->owner != s->ctx) return DPA_ERROR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(s->mutex);
+  // The worker and the finisher read fields[] without the lock: the vector
+  // never reallocates (its capacity is reserved at creation).
+  if (s->fields.size() == s->fields.capacity()) {
+    s->ctx->error = "server: at most " + std::to_string(kMaxServerFields) + " fields";
+    return DPA_ERROR_INVALID_ARGUMENT;
+  }
   s->fields.push_back(field);
   *id = int32_t(s->fields.size() - 1);
   return DPA_OK;
