@@ -5,7 +5,10 @@
 
 namespace dpa {
 
-constexpr int kAdvectBlock = 256;
+#ifndef DPA_ADVECT_BLOCK
+#define DPA_ADVECT_BLOCK 256
+#endif
+constexpr int kAdvectBlock = DPA_ADVECT_BLOCK;
 #ifndef DPA_ADVECT_MIN_BLOCKS
 #define DPA_ADVECT_MIN_BLOCKS 4
 #endif
