@@ -202,7 +202,7 @@ def cpu_baseline(a, grid, parts, target_seconds, steps_budget=None):
                       "OpenMP dynamic schedule standing in for TBB)"}
 
 
-def fp64_error(a, ctx, field, grid, parts, sample=512, horizons=(50, 250, None)):
+def fp64_error(a, ctx, field, grid, parts, sample=512, horizons=(50, 250, None), integrator=None):
     """Position error of the GPU path against the FP64 oracle integrator, in
     cells, over the first `sample` seeds that complete in both, at several
     horizons (the field is chaotic: FP32 and FP64 trajectories separate
@@ -213,11 +213,12 @@ def fp64_error(a, ctx, field, grid, parts, sample=512, horizons=(50, 250, None))
     ob.set_threads(os.cpu_count() or 1)
     og = ob.OracleGrid.of(grid)
     out = {"sample": sample}
-    adv = ParticleAdvector(ctx, sample, "none", a.integrator, a.step_size, False, False)
+    integrator = integrator or a.integrator
+    adv = ParticleAdvector(ctx, sample, "none", integrator, a.step_size, False, False)
     for h in horizons:
         h = a.iterations if h is None else min(h, a.iterations)
         gpu = adv.advect(field, Particles.create(parts.position[:sample], h)).inactive_particles
-        ref = ob.advect64(og, a.integrator, a.step_size, parts.position[:sample],
+        ref = ob.advect64(og, integrator, a.step_size, parts.position[:sample],
                           np.full(sample, h, np.uint64))
         ok = (ref.termination == 0) & (gpu.termination == 0)
         err = np.linalg.norm(gpu.position[ok].astype(np.float64) - ref.positions[ok], axis=1)
@@ -263,6 +264,37 @@ def precision_forms(a, ctx, grid, parts, p0, r0, pos, rem, term, stream, f32_ker
                         "fp64_error": fp64_error(a, ctx, field, grid, parts, horizons=(50, 250))}
         field.close()
     return out
+
+
+def true_rk4(a, ctx, field, grid, parts, p0, r0, pos, rem, term, stream, steps=3):
+    """The same workload with runge_kutta_4_true: four field samples per step
+    (the reference's runge_kutta_4 takes one, its system ignoring the state),
+    so four times the gathers; throughput and error against the FP64 oracle's
+    four-sample RK4."""
+    import ctypes as C
+    from dpa_b200 import _native as N
+    lib = ctx._lib
+    opts = N.AdvectOptions(N.INTEGRATORS["runge_kutta_4_true"], float(np.float32(a.step_size)),
+                           0, 0, 0, 1)
+    times = []
+    for i in range(steps + 1):
+        pos.copy_(p0)
+        rem.copy_(r0)
+        ctx.check(lib.dpa_advect_device(ctx.handle, field.handle, C.byref(opts), a.seeds,
+                                        C.c_void_p(pos.data_ptr()), C.c_void_p(rem.data_ptr()),
+                                        C.c_void_p(term.data_ptr()),
+                                        C.c_void_p(stream.cuda_stream)))
+        o, k = C.c_float(), C.c_float()
+        ctx.check(lib.dpa_context_last_timing(ctx.handle, C.byref(o), C.byref(k)))
+        if i:
+            times.append(k.value)
+    taken = float((a.iterations - rem.cpu().numpy().astype(np.int64)).sum())
+    kernel = statistics.mean(times)
+    return {"field_samples_per_step": 4, "kernel_ms": kernel,
+            "particle_steps_per_s": taken / (kernel / 1e3),
+            "algorithmic_bytes_per_step": 4 * BYTES_PER_STEP[a.storage],
+            "fp64_error": fp64_error(a, ctx, field, grid, parts, horizons=(50, 250),
+                                     integrator="runge_kutta_4_true")}
 
 
 def _graph_replays(ctx, field, opts, p0, r0, pos, rem, term, stream, steps):
@@ -713,6 +745,8 @@ def run_gpu(a):
         out["fp64_error"] = fp64_error(a, ctx, field, grid, parts)
         out["precision_forms"] = precision_forms(a, ctx, grid, parts, pristine_pos, pristine_rem,
                                                  pos, rem, term, stream, statistics.mean(kernel_ms))
+        out["true_rk4"] = true_rk4(a, ctx, field, grid, parts, pristine_pos, pristine_rem, pos,
+                                   rem, term, stream)
         if not a.no_systems:
             out["systems_forms"] = systems_forms(a, ctx, grid, pristine_pos, pristine_rem, pos, rem,
                                                  term, stream, ms_max)

@@ -44,7 +44,10 @@ struct CurveCounter {
 // counter per stretch (a stretch ends at 2^32 - 1 steps at the latest).
 template <int kIntegrator, int kStorage, bool kPow2, bool kRecord, bool kUnsteady>
 __global__ void __launch_bounds__(kAdvectBlock,
-                                  kUnsteady ? kAdvectUnsteadyMinBlocks : kAdvectMinBlocks)
+                                  kUnsteady ? kAdvectUnsteadyMinBlocks
+                                  : kIntegrator == DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE
+                                      ? kAdvectTrueRk4MinBlocks
+                                      : kAdvectMinBlocks)
 advect_kernel(const FieldView f, const AdvectArgs a) {
   using Sampler = std::conditional_t<kUnsteady, TimeSampler<kStorage, kPow2>,
                                      CellSampler<kStorage, kPow2>>;

@@ -19,6 +19,12 @@ constexpr int kAdvectMinBlocks = DPA_ADVECT_MIN_BLOCKS;
 #define DPA_ADVECT_UNSTEADY_MIN_BLOCKS 2
 #endif
 constexpr int kAdvectUnsteadyMinBlocks = DPA_ADVECT_UNSTEADY_MIN_BLOCKS;
+// Four-sample RK4 keeps three more stage derivatives alive: up to 80
+// registers (3 blocks per SM) instead of spilling at 64.
+#ifndef DPA_ADVECT_TRUE_RK4_MIN_BLOCKS
+#define DPA_ADVECT_TRUE_RK4_MIN_BLOCKS 3
+#endif
+constexpr int kAdvectTrueRk4MinBlocks = DPA_ADVECT_TRUE_RK4_MIN_BLOCKS;
 
 struct AdvectArgs {
   uint64_t count;
