@@ -835,6 +835,60 @@ def recording_at_scale(ctx, a, n=262144, iterations=2000):
     return out
 
 
+def ftle_fp64_error(grid, lattice, ftle_by_storage, iterations, step, lo=60, m=16):
+    """FTLE error against the FP64 oracle on an m^3 block of interior lattice
+    cells starting at lattice index lo (clear of the planes where the
+    reference's cell mapping collides): the block and a one-cell halo are
+    advected in double (the reference's one-sample RK4), the flow-map
+    Jacobian is taken by central differences over the lattice spacing, and
+    FTLE = ln sqrt(lambda_max(J^T J)) / |step * iterations|. Returns the
+    relative error of each storage's GPU FTLE over the block."""
+    from oracle import binding as ob
+    ob.build()
+    ob.set_threads(os.cpu_count() or 1)
+    n = 128
+    idx = np.arange(lo - 1, lo + m + 1)
+    ii, jj, kk = np.meshgrid(idx, idx, idx, indexing="ij")
+    flat = (ii * n + jj) * n + kk
+    seeds = lattice[flat.reshape(-1)]
+    r = ob.advect64(ob.OracleGrid.of(grid), "runge_kutta_4", step, seeds,
+                    np.full(len(seeds), iterations, np.uint64))
+    flow = r.positions.reshape(m + 2, m + 2, m + 2, 3)
+    h = 2.0 * np.asarray(grid.spacing, np.float64) * 2.0  # central difference over 2 lattice cells
+    J = np.stack([(flow[2:, 1:-1, 1:-1] - flow[:-2, 1:-1, 1:-1]) / h[0],
+                  (flow[1:-1, 2:, 1:-1] - flow[1:-1, :-2, 1:-1]) / h[1],
+                  (flow[1:-1, 1:-1, 2:] - flow[1:-1, 1:-1, :-2]) / h[2]], axis=-1)
+    C = np.einsum("...ki,...kj->...ij", J, J)
+    lam = np.linalg.eigvalsh(C)[..., -1]
+    want = np.log(np.sqrt(lam)) / abs(float(np.float32(step) * np.float32(iterations)))
+    # Cells whose whole stencil ran every iteration without leaving the grid:
+    # elsewhere the flow map holds exit positions, which a one-step difference
+    # in the exit moves by a cell or more.
+    done = (r.termination == 0).reshape(m + 2, m + 2, m + 2)
+    inside = done[1:-1, 1:-1, 1:-1].copy()
+    for d, sl in enumerate([(slice(2, None), slice(1, -1), slice(1, -1)),
+                            (slice(None, -2), slice(1, -1), slice(1, -1)),
+                            (slice(1, -1), slice(2, None), slice(1, -1)),
+                            (slice(1, -1), slice(None, -2), slice(1, -1)),
+                            (slice(1, -1), slice(1, -1), slice(2, None)),
+                            (slice(1, -1), slice(1, -1), slice(None, -2))]):
+        inside &= done[sl]
+    out = {"block": f"lattice cells [{lo}, {lo + m})^3 of 128^3, FP64 reference-semantics RK4"}
+    for storage, ftle in ftle_by_storage.items():
+        got = ftle.reshape(n, n, n)[lo:lo + m, lo:lo + m, lo:lo + m].astype(np.float64)
+        ok = np.isfinite(want) & np.isfinite(got) & (np.abs(want) > 1e-6)
+        entry = {}
+        for name, mask in (("all_cells", ok), ("stencil_inside", ok & inside)):
+            if not mask.any():
+                entry[name] = {"cells": 0}
+                continue
+            rel = np.abs(got[mask] - want[mask]) / np.abs(want[mask])
+            entry[name] = {"cells": int(mask.sum()), "median_rel": float(np.median(rel)),
+                           "p99_rel": float(np.percentile(rel, 99)), "max_rel": float(rel.max())}
+        out[storage] = entry
+    return out
+
+
 def run_secondary(a):
     """The FTLE and recording configurations: device-timed steps through the
     device entry points (FTLE) or the host round with its curve (recording),
@@ -977,6 +1031,24 @@ def run_secondary(a):
 
         e2e_once()
         e2e = statistics.mean([e2e_once() for _ in range(3)])
+        # FTLE of the other storage on the same lattice, and both against
+        # the FP64 oracle on an interior block.
+        ftles = {a.storage: ftle.cpu().numpy()}
+        other = "f16" if a.storage == "f32" else "f32"
+        f2 = ctx.field(grid, other)
+        p.copy_(p0)
+        r.copy_(r0)
+        ctx.check(lib.dpa_advect_device(ctx.handle, f2.handle, C.byref(opts), n,
+                                        C.c_void_p(p.data_ptr()), C.c_void_p(r.data_ptr()),
+                                        C.c_void_p(term.data_ptr()),
+                                        C.c_void_p(stream.cuda_stream)))
+        ctx.check(lib.dpa_ftle_estimate_device(
+            ctx.handle, f2.handle, stride, iterations, float(np.float32(step)), n,
+            C.c_void_p(p0.data_ptr()), C.c_void_p(p.data_ptr()), 0,
+            C.c_void_p(ftle.data_ptr()), shape, C.c_void_p(stream.cuda_stream)))
+        ftles[other] = ftle.cpu().numpy()
+        f2.close()
+        out["ftle_fp64_error"] = ftle_fp64_error(grid, pos, ftles, iterations, step)
         out.update({
             "value": steps_taken / (ms / 1e3), "ms_per_step": ms,
             "particle_steps_per_step": steps_taken, "kernel_ms": kern,
