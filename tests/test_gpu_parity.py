@@ -228,3 +228,25 @@ def test_ftle_matches_oracle(ctx, oracle, mapping):
     finite = np.isfinite(want)
     np.testing.assert_array_equal(np.isfinite(got.data), finite)
     np.testing.assert_allclose(got.data[finite], want[finite], rtol=1e-3, atol=1e-6)
+
+
+def test_degenerate_and_anisotropic_grids(ctx, oracle):
+    rng = np.random.default_rng(12)
+    # One cell (2 x 2 x 2 nodes); an axis of a single node (no cell is inside);
+    # an anisotropic grid with a negative offset and mixed spacings, one of
+    # them a power of two; power-of-two spacings with non-zero offsets.
+    cases = [
+        (rng.normal(size=(2, 2, 2, 3)).astype(np.float32), (0.5, 0.5, 0.5), (0.0, 0.0, 0.0)),
+        (rng.normal(size=(4, 1, 4, 3)).astype(np.float32), (1.0, 1.0, 1.0), (0.0, 0.0, 0.0)),
+        (rng.normal(size=(9, 5, 13, 3)).astype(np.float32), (0.3, 2.0, 0.125),
+         (-1.25, 3.0, -0.5)),
+        # power-of-two spacings with non-zero offsets: the one-FMA location
+        (rng.normal(size=(7, 11, 6, 3)).astype(np.float32), (0.5, 0.25, 2.0),
+         (-1.5, -0.75, 4.0)),
+    ]
+    for data, spacing, offset in cases:
+        grid = dpa_b200.RegularGrid.from_data(data, spacing, offset)
+        lo = np.asarray(offset, np.float32)
+        hi = lo + np.asarray(spacing, np.float32) * (np.asarray(data.shape[:3]) - 1)
+        pos = (lo + rng.random((300, 3)) * (hi - lo) * 1.02 - 0.01 * (hi - lo)).astype(np.float32)
+        compare(ctx, oracle, grid, pos, 40, "runge_kutta_4", 0.05, 300, True)
