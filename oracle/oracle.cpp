@@ -75,16 +75,17 @@ inline bool equals_sentinel(const float* v, float s) {
 // regular_grid<vector3, 3>
 // ---------------------------------------------------------------------------
 
-// regular_grid.hpp:41-50. Valid iff 0 <= floor((p - o) / h) <= n - 2 on
-// every axis. The reference converts the float subscript to int64 for the
-// lower test and to size_t for the upper one; on x86-64 both conversions
-// reject NaN and out-of-range values, which the float comparisons below
-// reproduce without the undefined conversions.
+// regular_grid.hpp:41-50. Valid iff 0 <= floor((p - o) / h) < n - 1 on
+// every axis (so an axis of one node holds no valid position). The reference
+// converts the float subscript to int64 for the lower test and to size_t for
+// the upper one, compared with shape - 1; on x86-64 both conversions reject
+// NaN and out-of-range values, which the float comparisons below reproduce
+// without the undefined conversions.
 bool grid_contains(const oracle_grid& g, const float* p) {
   for (int i = 0; i < 3; ++i) {
     const float subscript = std::floor((p[i] - g.offset[i]) / g.spacing[i]);
     if (!(subscript >= 0.0f)) return false;
-    if (!(subscript <= static_cast<float>(g.shape[i] - 2))) return false;
+    if (!(subscript < static_cast<float>(g.shape[i] - 1))) return false;
   }
   return true;
 }
@@ -306,7 +307,7 @@ struct unsteady_field {
   }
   bool contains(const float* p, float t) const {
     const float subscript = std::floor((t - u.time_origin) / u.time_spacing);
-    if (!(subscript >= 0.0f) || !(subscript <= static_cast<float>(u.slices - 2))) return false;
+    if (!(subscript >= 0.0f) || !(subscript < static_cast<float>(u.slices - 1))) return false;
     return grid_contains(slice(0), p);
   }
   void interpolate(const float* p, float t, float* out) const {
@@ -425,7 +426,7 @@ bool grid_contains64(const oracle_grid& g, const double* p) {
   for (int i = 0; i < 3; ++i) {
     const double s = std::floor((p[i] - double(g.offset[i])) / double(g.spacing[i]));
     if (!(s >= 0.0)) return false;
-    if (!(s <= double(g.shape[i] - 2))) return false;
+    if (!(s < double(g.shape[i] - 1))) return false;
   }
   return true;
 }

@@ -19,6 +19,14 @@ def test_contains_rule(oracle):
     assert oracle.contains(g, [-0.0, 0.5, 3])
     assert not oracle.contains(g, [np.nan, 0.5, 3])
     assert not oracle.contains(g, [np.inf, 0.5, 3])
+    # An axis of one node has no cell (the reference compares the subscript
+    # with shape - 1 = 0), so nothing is inside such a grid.
+    flat = oracle.OracleGrid(np.zeros((4, 1, 4, 3), np.float32), (1, 1, 1))
+    assert not oracle.contains(flat, [1.0, 0.0, 1.0])
+    assert not oracle.contains(flat, [1.0, -0.0, 1.0])
+    one = oracle.OracleGrid(np.zeros((2, 2, 2, 3), np.float32), (1, 1, 1))
+    assert oracle.contains(one, [0.5, 0.5, 0.999])
+    assert not oracle.contains(one, [0.5, 0.5, 1.0])
 
 
 def test_trilinear_is_exact_on_linear_fields(oracle):
