@@ -226,7 +226,8 @@ def fp64_error(a, ctx, field, grid, parts, sample=512, horizons=(50, 250, None),
         out[f"steps_{h}"] = {
             "completed": int(ok.sum()),
             "median_cells": float(np.median(err)) if ok.any() else None,
-            "max_cells": float(np.max(err)) if ok.any() else None}
+            "max_cells": float(np.max(err)) if ok.any() else None,
+            "within_1e-3_cells": float(np.mean(err <= 1e-3)) if ok.any() else None}
     return out
 
 
