@@ -153,7 +153,8 @@ __global__ void set_steps_kernel(const uint64_t* in, const uint64_t* out, const 
 }
 
 __global__ void expand_ranges_kernel(const uint64_t* starts, const uint64_t* firsts,
-                                     uint32_t ranges, uint64_t total, uint32_t* list) {
+                                     uint32_t ranges, uint64_t total, const uint32_t* order,
+                                     uint32_t* list) {
   const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= total) return;
   uint32_t lo = 0, hi = ranges;  // last range whose first entry is <= t
@@ -162,16 +163,18 @@ __global__ void expand_ranges_kernel(const uint64_t* starts, const uint64_t* fir
     if (firsts[mid] <= t) lo = mid;
     else hi = mid;
   }
-  list[t] = uint32_t(starts[lo] + (t - firsts[lo]));
+  const uint64_t start = starts[lo];
+  list[t] = uint32_t(start + order[start + (t - firsts[lo])]);
 }
 
 }  // namespace
 
 cudaError_t launch_expand_ranges(const uint64_t* starts, const uint64_t* firsts, uint32_t ranges,
-                                 uint64_t total, uint32_t* list, cudaStream_t stream) {
+                                 uint64_t total, const uint32_t* order, uint32_t* list,
+                                 cudaStream_t stream) {
   if (total == 0 || ranges == 0) return cudaSuccess;
   expand_ranges_kernel<<<unsigned((total + 255) / 256), 256, 0, stream>>>(starts, firsts, ranges,
-                                                                          total, list);
+                                                                          total, order, list);
   return cudaGetLastError();
 }
 

@@ -65,10 +65,13 @@ inline void set_launch_defaults(AdvectArgs& a) {
   a.in_flight = nullptr;
 }
 
-// list[t] = starts[r] + (t - firsts[r]) for the range r holding t, where
-// firsts is the exclusive scan of the range lengths (ranges of arena slots).
+// list[t] = starts[r] + order[starts[r] + (t - firsts[r])] for the range r
+// holding t, where firsts is the exclusive scan of the range lengths (ranges
+// of arena slots) and order holds, per slot, a permutation of each range's
+// offsets (its processing order).
 cudaError_t launch_expand_ranges(const uint64_t* starts, const uint64_t* firsts, uint32_t ranges,
-                                 uint64_t total, uint32_t* list, cudaStream_t stream);
+                                 uint64_t total, const uint32_t* order, uint32_t* list,
+                                 cudaStream_t stream);
 
 // Picks the kernel instantiation for the field (steady or time-varying,
 // storage, power-of-two spacing), the integrator and recording.

@@ -122,6 +122,10 @@ struct dpa_server {
   // Particle arena (per slot) and curve staging arena (per vertex).
   DeviceBuffer positions, times, remaining, remaining_initial, termination, raw_offsets,
       kept_vertices, kept_segments, curve_open, request_of, raw, in_flight;
+  // Processing order of each request's particles, relative to its first slot
+  // (a Morton sort of its seeds at admission), and the sort's bucket ids and
+  // counters.
+  DeviceBuffer seed_order, order_ids, order_counts;
   // Per tick. Two ticks may be in flight, so the host-side buffers a tick's
   // copies read or write come in two halves, one per tick parity.
   DeviceBuffer list, starts, firsts, work_counter;
@@ -187,10 +191,11 @@ namespace {
 // `slot`, at time t0, with curve staging at raw_first + i (iterations + 2);
 // the request's in-flight counter = n.
 __global__ void serve_init_kernel(uint64_t first, uint64_t n, uint64_t iterations, float t0,
-                                  uint32_t slot, bool record, uint64_t raw_first,
+                                  uint32_t slot, bool record, uint64_t raw_first, bool ordered,
                                   uint64_t* remaining, uint64_t* remaining_initial,
                                   uint8_t* termination, uint32_t* request_of, float* times,
-                                  uint64_t* raw_offsets, unsigned int* in_flight) {
+                                  uint64_t* raw_offsets, uint32_t* seed_order,
+                                  unsigned int* in_flight) {
   const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i == 0) in_flight[slot] = unsigned(n);
   if (i >= n) return;
@@ -201,7 +206,12 @@ __global__ void serve_init_kernel(uint64_t first, uint64_t n, uint64_t iteration
   request_of[k] = slot;
   times[k] = t0;
   if (record) raw_offsets[k] = raw_first + i * (iterations + 2);
+  if (!ordered) seed_order[k] = uint32_t(i);
 }
+
+// Requests of fewer seeds run in submission order: sorting them would cost
+// more launches than their few warps gain in locality.
+constexpr uint64_t kServeOrderMin = 4096;
 
 // Requests advance in step budgets of steps_per_tick, so a particle resumes
 // in a later tick: integrators that carry a derivative from one step to the
@@ -244,10 +254,11 @@ void dpa_server::select(std::vector<active_request>& out) {
 // Starts admitted requests on the device: their seeds are copied in on the
 // upload stream, beside the running tick (whose particles never share slots
 // with them: a slot is reused only after its request has finished and been
-// returned, and ticks skip finished particles); then, in the ticks' stream
-// order, an init kernel per request sets its per-particle state (every
-// particle in flight) and its in-flight counter. Worker thread, without the
-// mutex.
+// returned, and ticks skip finished particles), and sorted there into their
+// processing order, so that the lanes of a tick sweep each request's seeds
+// in Morton order of their start cells; then, in the ticks' stream order, an
+// init kernel per request sets its per-particle state (every particle in
+// flight) and its in-flight counter. Worker thread, without the mutex.
 void dpa_server::upload(std::vector<active_request>& admitted, uint64_t first_tick) {
   for (active_request& a : admitted) {
     a.first_tick = first_tick;
@@ -255,6 +266,13 @@ void dpa_server::upload(std::vector<active_request>& admitted, uint64_t first_ti
     if (n)
       SERVER_TRY(cudaMemcpyAsync(positions.as<float>() + 3 * a.first, a.p.positions.data(),
                                  n * 12, cudaMemcpyHostToDevice, upload_stream));
+    if (n >= kServeOrderMin && ctx->tuning.order)
+      SERVER_TRY(dpa::launch_order(fields[size_t(a.p.request.field)]->view,
+                                   positions.as<float>() + 3 * a.first, n,
+                                   order_ids.as<uint32_t>() + a.first,
+                                   order_counts.as<uint32_t>(),
+                                   seed_order.as<uint32_t>() + a.first, upload_stream,
+                                   ctx->tuning.order));
   }
   SERVER_TRY(cudaEventRecord(seeds_copied, upload_stream));
   SERVER_TRY(cudaStreamWaitEvent(stream, seeds_copied, 0));
@@ -263,8 +281,9 @@ void dpa_server::upload(std::vector<active_request>& admitted, uint64_t first_ti
     const uint64_t n = q.count;
     serve_init_kernel<<<unsigned(std::max<uint64_t>((n + 255) / 256, 1)), 256, 0, stream>>>(
         a.first, n, q.iterations, q.start_time, a.slot, q.record != 0, a.raw_first,
-        remaining.as<uint64_t>(), remaining_initial.as<uint64_t>(), termination.as<uint8_t>(),
-        request_of.as<uint32_t>(), times.as<float>(), raw_offsets.as<uint64_t>(),
+        n >= kServeOrderMin && ctx->tuning.order, remaining.as<uint64_t>(),
+        remaining_initial.as<uint64_t>(), termination.as<uint8_t>(), request_of.as<uint32_t>(),
+        times.as<float>(), raw_offsets.as<uint64_t>(), seed_order.as<uint32_t>(),
         in_flight.as<unsigned int>());
     SERVER_TRY(cudaGetLastError());
   }
@@ -308,7 +327,8 @@ uint32_t dpa_server::tick(uint64_t steps, int parity) {
     SERVER_TRY(cudaMemcpyAsync(firsts.ptr, h + ranges, uint64_t(ranges) * 8, cudaMemcpyHostToDevice,
                                stream));
     SERVER_TRY(dpa::launch_expand_ranges(starts.as<uint64_t>(), firsts.as<uint64_t>(), ranges,
-                                         total, list.as<uint32_t>(), stream));
+                                         total, seed_order.as<uint32_t>(), list.as<uint32_t>(),
+                                         stream));
     dpa::AdvectArgs a{};
     dpa::set_launch_defaults(a);
     a.count = total;
@@ -646,9 +666,11 @@ int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_s
     cudaError_t e = cudaSuccess;
     DeviceBuffer* per_slot[] = {&s->positions, &s->times, &s->remaining, &s->remaining_initial,
                                 &s->termination, &s->raw_offsets, &s->kept_vertices,
-                                &s->kept_segments, &s->curve_open, &s->request_of};
-    const size_t bytes[] = {12, 4, 8, 8, 1, 8, 4, 4, 1, 4};
-    for (size_t i = 0; i < 10 && e == cudaSuccess; ++i) e = per_slot[i]->reserve(p * bytes[i]);
+                                &s->kept_segments, &s->curve_open, &s->request_of,
+                                &s->seed_order, &s->order_ids};
+    const size_t bytes[] = {12, 4, 8, 8, 1, 8, 4, 4, 1, 4, 4, 4};
+    for (size_t i = 0; i < 12 && e == cudaSuccess; ++i) e = per_slot[i]->reserve(p * bytes[i]);
+    if (e == cudaSuccess) e = s->order_counts.reserve(dpa::kOrderCountsSize * 4);
     if (e == cudaSuccess) e = s->raw.reserve(std::max<uint64_t>(v, 1) * 12);
     if (e == cudaSuccess) e = s->in_flight.reserve(4 * uint64_t(options->max_requests));
     if (e == cudaSuccess) e = s->work_counter.reserve(8);

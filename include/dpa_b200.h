@@ -292,11 +292,13 @@ int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_adve
  * sharing a field, integrator, step size and recording switch. Requests that
  * arrive while others run join at the next tick. A worker thread owns the
  * ticks; a second thread, on its own stream, copies out, emits and returns
- * the requests that have finished while the ticks go on. submit, poll and
- * stats may be called from any thread. The context is used for its device
- * and its fields only. */
+ * the requests that have finished while the ticks go on. A request of 4096
+ * seeds or more is swept in the Morton order of its seeds' start cells (the
+ * context's tuning order; submission order when that is off). submit, poll
+ * and stats may be called from any thread. The context is used for its
+ * device, its fields and its tuning only. */
 typedef struct dpa_server_options {
-  uint64_t particle_capacity;  /* particle slots of the arena */
+  uint64_t particle_capacity;  /* particle slots of the arena (62 bytes each) */
   uint64_t vertex_capacity;    /* curve-staging vertices of the arena (12 bytes each) */
   uint32_t steps_per_tick;     /* step budget of a tick while requests wait for
                                   admission (0: 64); four times as many while

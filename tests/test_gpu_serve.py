@@ -1,6 +1,8 @@
 """The request server: every result is the same alone and in a mix of
 concurrent requests (bit for bit), requests that do not fit wait for room,
-and requests that can never fit are refused."""
+and requests that can never fit are refused. The mix holds requests of 4096
+seeds or more, which the server sweeps in the Morton order of their seeds,
+and smaller ones, swept in submission order."""
 import math
 import time
 
