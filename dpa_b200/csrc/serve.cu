@@ -254,11 +254,15 @@ void dpa_server::select(std::vector<active_request>& out) {
 // Starts admitted requests on the device: their seeds are copied in on the
 // upload stream, beside the running tick (whose particles never share slots
 // with them: a slot is reused only after its request has finished and been
-// returned, and ticks skip finished particles), and sorted there into their
-// processing order, so that the lanes of a tick sweep each request's seeds
-// in Morton order of their start cells; then, in the ticks' stream order, an
-// init kernel per request sets its per-particle state (every particle in
-// flight) and its in-flight counter. Worker thread, without the mutex.
+// returned, and ticks skip finished particles). Then, in the ticks' stream
+// order, a request of kServeOrderMin seeds or more is sorted into its
+// processing order, so that the lanes of a tick sweep its seeds in Morton
+// order of their start cells, and an init kernel per request sets its
+// per-particle state (every particle in flight) and its in-flight counter.
+// The sort stays in the ticks' stream: a running tick may still expand the
+// slot range of a request that finished in the tick before (ticks skip its
+// particles, but read its processing order), and a new request may reuse
+// that range. Worker thread, without the mutex.
 void dpa_server::upload(std::vector<active_request>& admitted, uint64_t first_tick) {
   for (active_request& a : admitted) {
     a.first_tick = first_tick;
@@ -266,16 +270,19 @@ void dpa_server::upload(std::vector<active_request>& admitted, uint64_t first_ti
     if (n)
       SERVER_TRY(cudaMemcpyAsync(positions.as<float>() + 3 * a.first, a.p.positions.data(),
                                  n * 12, cudaMemcpyHostToDevice, upload_stream));
+  }
+  SERVER_TRY(cudaEventRecord(seeds_copied, upload_stream));
+  SERVER_TRY(cudaStreamWaitEvent(stream, seeds_copied, 0));
+  for (const active_request& a : admitted) {
+    const uint64_t n = a.p.request.count;
     if (n >= kServeOrderMin && ctx->tuning.order)
       SERVER_TRY(dpa::launch_order(fields[size_t(a.p.request.field)]->view,
                                    positions.as<float>() + 3 * a.first, n,
                                    order_ids.as<uint32_t>() + a.first,
                                    order_counts.as<uint32_t>(),
-                                   seed_order.as<uint32_t>() + a.first, upload_stream,
+                                   seed_order.as<uint32_t>() + a.first, stream,
                                    ctx->tuning.order));
   }
-  SERVER_TRY(cudaEventRecord(seeds_copied, upload_stream));
-  SERVER_TRY(cudaStreamWaitEvent(stream, seeds_copied, 0));
   for (const active_request& a : admitted) {
     const dpa_request& q = a.p.request;
     const uint64_t n = q.count;
