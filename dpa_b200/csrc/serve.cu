@@ -727,11 +727,12 @@ int dpa_server_submit(dpa_server* s, const dpa_request* request, uint64_t* id) {
   }
   if (!integrator_ok(q.integrator)) return DPA_ERROR_UNSUPPORTED;
   if (q.count && !q.positions) return DPA_ERROR_INVALID_ARGUMENT;
+  // The range checks come first: they bound count * (iterations + 2) below 2^64.
+  if (q.count > 0xffffffffull) return DPA_ERROR_INVALID_ARGUMENT;
+  if (q.record && q.iterations > 0xfffffff0ull) return DPA_ERROR_INVALID_ARGUMENT;
   if (q.count > s->options.particle_capacity) return DPA_ERROR_OUT_OF_MEMORY;
   if (q.record && q.count * (q.iterations + 2) > s->options.vertex_capacity)
     return DPA_ERROR_OUT_OF_MEMORY;
-  if (q.record && q.iterations > 0xfffffff0ull) return DPA_ERROR_INVALID_ARGUMENT;
-  if (q.count > 0xffffffffull) return DPA_ERROR_INVALID_ARGUMENT;
   try {
     pending p;
     p.request = q;
