@@ -50,7 +50,7 @@ def _run(cmd: list[str]) -> None:
 
 def build_library(force: bool = False, verbose_ptxas: bool = False) -> Path:
     sources = [CSRC / s for s in CUDA_SOURCES]
-    deps = sources + list(CSRC.glob("*.cuh")) + [INCLUDE / "dpa_b200.h"]
+    deps = sources + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.hpp")) + [INCLUDE / "dpa_b200.h"]
     if not force and not _stale(LIBRARY, deps):
         return LIBRARY
     build_dir = PACKAGE / "_build"

@@ -31,6 +31,7 @@
 
 #include "handles.cuh"
 #include "kernels.cuh"
+#include "range_allocator.hpp"
 
 namespace {
 
@@ -38,53 +39,7 @@ using clock_type = std::chrono::steady_clock;
 
 constexpr size_t kMaxServerFields = 256;
 
-// First-fit allocator of [0, capacity) ranges, coalescing on free.
-class range_allocator {
- public:
-  explicit range_allocator(uint64_t capacity = 0) { reset(capacity); }
-  void reset(uint64_t capacity) {
-    free_.clear();
-    if (capacity) free_[0] = capacity;
-    capacity_ = capacity;
-  }
-  bool allocate(uint64_t n, uint64_t* offset) {
-    if (n == 0) {
-      *offset = 0;
-      return true;
-    }
-    for (auto it = free_.begin(); it != free_.end(); ++it) {
-      if (it->second >= n) {
-        *offset = it->first;
-        const uint64_t rest = it->second - n;
-        const uint64_t at = it->first + n;
-        free_.erase(it);
-        if (rest) free_[at] = rest;
-        return true;
-      }
-    }
-    return false;
-  }
-  void release(uint64_t offset, uint64_t n) {
-    if (n == 0) return;
-    auto next = free_.lower_bound(offset);
-    if (next != free_.end() && offset + n == next->first) {
-      n += next->second;
-      next = free_.erase(next);
-    }
-    if (next != free_.begin()) {
-      auto prev = std::prev(next);
-      if (prev->first + prev->second == offset) {
-        prev->second += n;
-        return;
-      }
-    }
-    free_[offset] = n;
-  }
-
- private:
-  std::map<uint64_t, uint64_t> free_;
-  uint64_t capacity_ = 0;
-};
+using dpa::range_allocator;
 
 struct pending {
   uint64_t id;

@@ -1,0 +1,106 @@
+"""CPU tests of the request server's host logic: the first-fit range allocator
+behind its particle-slot and curve-staging arenas, compiled on its own and
+checked against a slot-by-slot model (no GPU needed)."""
+import shutil
+import subprocess
+from pathlib import Path
+
+import pytest
+
+CSRC = Path(__file__).resolve().parent.parent / "dpa_b200" / "csrc"
+
+DRIVER = r"""
+#include <cstdio>
+#include <random>
+#include <vector>
+#include "range_allocator.hpp"
+
+// The model: one flag per entry. allocate must return the lowest offset
+// starting n free entries, or fail when no such run exists; release must make
+// the range whole again (adjacent free ranges merge).
+static bool fits_at(const std::vector<char>& used, uint64_t at, uint64_t n) {
+  for (uint64_t i = at; i < at + n; ++i) if (used[i]) return false;
+  return true;
+}
+static long lowest_fit(const std::vector<char>& used, uint64_t n) {
+  for (uint64_t at = 0; at + n <= used.size(); ++at) if (fits_at(used, at, n)) return long(at);
+  return -1;
+}
+
+int main() {
+  for (unsigned seed = 0; seed < 40; ++seed) {
+    std::mt19937_64 rng(seed);
+    const uint64_t capacity = 1 + rng() % 400;
+    dpa::range_allocator a(capacity);
+    std::vector<char> used(capacity, 0);
+    std::vector<std::pair<uint64_t, uint64_t>> live;
+    for (int op = 0; op < 3000; ++op) {
+      if (live.empty() || rng() % 5 < 3) {
+        const uint64_t n = rng() % (capacity / 3 + 2);
+        uint64_t at = 0;
+        const bool ok = a.allocate(n, &at);
+        const long want = n == 0 ? 0 : lowest_fit(used, n);
+        if (ok != (want >= 0) || (ok && long(at) != want)) {
+          std::printf("seed %u op %d: allocate(%llu) gave %d at %llu, model %ld\n", seed, op,
+                      (unsigned long long)n, int(ok), (unsigned long long)at, want);
+          return 1;
+        }
+        if (ok && n) {
+          for (uint64_t i = at; i < at + n; ++i) used[i] = 1;
+          live.push_back({at, n});
+        }
+      } else {
+        const size_t k = rng() % live.size();
+        a.release(live[k].first, live[k].second);
+        for (uint64_t i = live[k].first; i < live[k].first + live[k].second; ++i) used[i] = 0;
+        live.erase(live.begin() + long(k));
+      }
+      // Free ranges are maximal and match the model exactly.
+      uint64_t expect = 0;
+      long prev_end = -1;
+      for (const auto& r : a.free_ranges()) {
+        if (long(r.first) == prev_end || r.second == 0) {
+          std::printf("seed %u op %d: free ranges not merged at %llu\n", seed, op,
+                      (unsigned long long)r.first);
+          return 1;
+        }
+        for (uint64_t i = r.first; i < r.first + r.second; ++i) {
+          if (i >= capacity || used[i]) {
+            std::printf("seed %u op %d: entry %llu free in the allocator, used in the model\n",
+                        seed, op, (unsigned long long)i);
+            return 1;
+          }
+        }
+        expect += r.second;
+        prev_end = long(r.first + r.second);
+      }
+      uint64_t model_free = 0;
+      for (char u : used) model_free += !u;
+      if (expect != model_free) {
+        std::printf("seed %u op %d: %llu free in the allocator, %llu in the model\n", seed, op,
+                    (unsigned long long)expect, (unsigned long long)model_free);
+        return 1;
+      }
+    }
+    for (const auto& r : live) a.release(r.first, r.second);
+    uint64_t at = 1;
+    if (!a.allocate(capacity, &at) || at != 0) {
+      std::printf("seed %u: the emptied arena does not hold its capacity\n", seed);
+      return 1;
+    }
+  }
+  std::puts("ok");
+  return 0;
+}
+"""
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no C++ compiler")
+def test_range_allocator_is_first_fit_and_merges_free_ranges(tmp_path):
+    src = tmp_path / "driver.cpp"
+    exe = tmp_path / "driver"
+    src.write_text(DRIVER)
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-I", str(CSRC), str(src), "-o", str(exe)],
+                   check=True)
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert run.returncode == 0 and run.stdout.strip() == "ok", run.stdout + run.stderr
