@@ -719,7 +719,9 @@ def run_gpu(a):
     achieved = algorithmic / kernel_s / 1e9
     traffic = None
     tf = ROOT / "profiles" / "advect_traffic.json"
-    if tf.exists():
+    # The captured traffic is that of the default workload's launch (1,048,576
+    # seeds x 2000 iterations of step 0.25); other workloads have none.
+    if tf.exists() and a.seeds == 1 << 20 and a.iterations == 2000 and a.step_size == 0.25:
         try:
             traffic = json.loads(tf.read_text()).get(f"{a.storage}_{a.integrator}_n{a.n}")
         except Exception:
