@@ -8,6 +8,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <new>
 #include <string>
 #include <vector>
@@ -19,7 +20,8 @@ struct dpa_graph {
   dpa_context* owner = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
-  uint64_t launches = 0;  // kernels per replay
+  uint64_t launches = 0;        // kernels per replay
+  dpa_launch_scratch scratch;   // the captured launches' own scratch
 };
 
 namespace {
@@ -108,19 +110,20 @@ int check_options(dpa_context* ctx, const dpa_advect_options* o) {
 }
 
 // Builds the processing order of `count` device positions (coarse Morton
-// buckets, see launch_order) in ctx->values. Returns it through *order.
-int build_order(dpa_context* ctx, const dpa_field* field, const float* positions, uint64_t count,
-                cudaStream_t stream, const uint32_t** order) {
+// buckets, see launch_order) in scratch.values. Returns it through *order.
+int build_order(dpa_context* ctx, dpa_launch_scratch& scratch, const dpa_field* field,
+                const float* positions, uint64_t count, cudaStream_t stream,
+                const uint32_t** order) {
   *order = nullptr;
   if (count < 2) return DPA_OK;
-  DPA_TRY_CUDA(ctx, ctx->keys.reserve(count * 4));
-  DPA_TRY_CUDA(ctx, ctx->values.reserve(count * 4));
-  DPA_TRY_CUDA(ctx, ctx->sort_temp.reserve(dpa::kOrderCountsSize * 4));
-  DPA_TRY_CUDA(ctx, dpa::launch_order(field->view, positions, count, ctx->keys.as<uint32_t>(),
-                                      ctx->sort_temp.as<uint32_t>(), ctx->values.as<uint32_t>(),
-                                      stream, ctx->tuning.order));
+  DPA_TRY_CUDA(ctx, scratch.keys.reserve(count * 4));
+  DPA_TRY_CUDA(ctx, scratch.values.reserve(count * 4));
+  DPA_TRY_CUDA(ctx, scratch.sort_temp.reserve(dpa::kOrderCountsSize * 4));
+  DPA_TRY_CUDA(ctx, dpa::launch_order(field->view, positions, count, scratch.keys.as<uint32_t>(),
+                                      scratch.sort_temp.as<uint32_t>(),
+                                      scratch.values.as<uint32_t>(), stream, ctx->tuning.order));
   ctx->launches += dpa::kOrderLaunches;
-  *order = ctx->values.as<uint32_t>();
+  *order = scratch.values.as<uint32_t>();
   return DPA_OK;
 }
 
@@ -135,28 +138,32 @@ int check_steady(dpa_context* ctx, const dpa_field* field) {
 
 // Order (optional) + advection kernel over device arrays, no recording.
 // times (may be null for a steady field) are the particles' times.
+// The processing order and the advection launch for device arrays, with the
+// context's scratch or, for a graph's capture, the graph's own.
 int advect_device_impl(dpa_context* ctx, const dpa_field* field, const dpa_advect_options* o,
                        uint64_t count, float* positions, uint64_t* remaining, uint8_t* termination,
-                       cudaStream_t s, float* times = nullptr) {
+                       cudaStream_t s, float* times = nullptr,
+                       dpa_launch_scratch* own_scratch = nullptr) {
   if (!times) {
     const int st = check_steady(ctx, field);
     if (st != DPA_OK) return st;
   }
   if (count == 0) return DPA_OK;
+  dpa_launch_scratch& scratch = own_scratch ? *own_scratch : ctx->scratch;
   if (ctx->profiling) DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->events[0], s));
   const uint32_t* order = nullptr;
   if (o->morton_order && ctx->tuning.order) {
-    const int st = build_order(ctx, field, positions, count, s, &order);
+    const int st = build_order(ctx, scratch, field, positions, count, s, &order);
     if (st != DPA_OK) return st;
   }
   if (ctx->profiling) DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->events[1], s));
-  DPA_TRY_CUDA(ctx, ctx->work_counter.reserve(sizeof(unsigned long long)));
+  DPA_TRY_CUDA(ctx, scratch.work_counter.reserve(sizeof(unsigned long long)));
   dpa::AdvectArgs a{};
   dpa::set_launch_defaults(a);
   if (o->max_steps) a.max_steps = o->max_steps;
   a.claim = ctx->tuning.claim;
   a.blocks_per_sm = ctx->tuning.blocks_per_sm;
-  a.work_counter = ctx->work_counter.as<unsigned long long>();
+  a.work_counter = scratch.work_counter.as<unsigned long long>();
   a.count = count;
   a.order = order;
   a.positions = positions;
@@ -216,15 +223,15 @@ int record_piece(dpa_context* ctx, const dpa_field* field, const dpa_advect_opti
   uint8_t* termination = ctx->termination.as<uint8_t>() + begin;
   const uint32_t* order = nullptr;
   if (o->morton_order && ctx->tuning.order) {
-    const int st = build_order(ctx, field, positions, n, s, &order);
+    const int st = build_order(ctx, ctx->scratch, field, positions, n, s, &order);
     if (st != DPA_OK) return st;
   }
-  DPA_TRY_CUDA(ctx, ctx->work_counter.reserve(sizeof(unsigned long long)));
+  DPA_TRY_CUDA(ctx, ctx->scratch.work_counter.reserve(sizeof(unsigned long long)));
   dpa::AdvectArgs a{};
   dpa::set_launch_defaults(a);
   a.claim = ctx->tuning.claim;
   a.blocks_per_sm = ctx->tuning.blocks_per_sm;
-  a.work_counter = ctx->work_counter.as<unsigned long long>();
+  a.work_counter = ctx->scratch.work_counter.as<unsigned long long>();
   a.count = n;
   a.order = order;
   a.positions = positions;
@@ -1041,11 +1048,15 @@ int dpa_graph_create_advect(dpa_context* ctx, const dpa_field* field,
   return guarded(ctx, [&]() -> int {
     DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
     cudaStream_t s = ctx->stream;
+    auto g = std::make_unique<dpa_graph>();
+    g->owner = ctx;
     // Everything the launch sequence allocates or looks up, before capture.
-    DPA_TRY_CUDA(ctx, ctx->keys.reserve(count * 4));
-    DPA_TRY_CUDA(ctx, ctx->values.reserve(count * 4));
-    DPA_TRY_CUDA(ctx, ctx->sort_temp.reserve(dpa::kOrderCountsSize * 4));
-    DPA_TRY_CUDA(ctx, ctx->work_counter.reserve(sizeof(unsigned long long)));
+    // The graph's scratch is its own: the captured kernels keep its
+    // addresses for every replay.
+    DPA_TRY_CUDA(ctx, g->scratch.keys.reserve(count * 4));
+    DPA_TRY_CUDA(ctx, g->scratch.values.reserve(count * 4));
+    DPA_TRY_CUDA(ctx, g->scratch.sort_temp.reserve(dpa::kOrderCountsSize * 4));
+    DPA_TRY_CUDA(ctx, g->scratch.work_counter.reserve(sizeof(unsigned long long)));
     DPA_TRY_CUDA(ctx, dpa::prepare_advect(field->view, options->integrator, false));
     DPA_TRY_CUDA(ctx, cudaStreamSynchronize(s));
     const bool profiling = ctx->profiling;
@@ -1054,9 +1065,11 @@ int dpa_graph_create_advect(dpa_context* ctx, const dpa_field* field,
     cudaGraph_t graph = nullptr;
     DPA_TRY_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
     st = advect_device_impl(ctx, field, options, count, device_positions, device_remaining,
-                            device_termination, s);
+                            device_termination, s, nullptr, &g->scratch);
     const cudaError_t end = cudaStreamEndCapture(s, &graph);
     ctx->profiling = profiling;
+    const uint64_t captured = ctx->launches - launches0;
+    ctx->launches = launches0;  // capture launched nothing
     if (st != DPA_OK) {
       if (graph) cudaGraphDestroy(graph);
       return st;
@@ -1068,13 +1081,10 @@ int dpa_graph_create_advect(dpa_context* ctx, const dpa_field* field,
       cudaGraphDestroy(graph);
       return fail_cuda(ctx, inst, "cudaGraphInstantiate");
     }
-    dpa_graph* g = new dpa_graph();
-    g->owner = ctx;
     g->graph = graph;
     g->exec = exec;
-    g->launches = ctx->launches - launches0;
-    ctx->launches = launches0;  // capture launched nothing
-    *out = g;
+    g->launches = captured;
+    *out = g.release();
     return DPA_OK;
   });
 }
@@ -1090,7 +1100,8 @@ int dpa_graph_launch(dpa_context* ctx, dpa_graph* graph, void* stream) {
 int dpa_graph_destroy(dpa_context* ctx, dpa_graph* graph) {
   if (!ctx || !graph || graph->owner != ctx) return DPA_ERROR_INVALID_ARGUMENT;
   cudaSetDevice(ctx->device);
-  cudaStreamSynchronize(ctx->stream);
+  // Replays may run on any stream; the scratch goes only once they are done.
+  cudaDeviceSynchronize();
   if (graph->exec) cudaGraphExecDestroy(graph->exec);
   if (graph->graph) cudaGraphDestroy(graph->graph);
   delete graph;

@@ -79,6 +79,20 @@ struct dpa_tuning_state {
                               // coarsening of the grid (1..64); 0: input order
 };
 
+// Scratch of one processing-order + advection launch sequence: bucket ids,
+// the order, the counting sort's counters and the claim counter. A context
+// keeps one for its calls; a CUDA graph keeps its own, because a later call
+// with more particles reallocates the context's.
+struct dpa_launch_scratch {
+  DeviceBuffer keys, values, sort_temp, work_counter;
+  void release() {
+    keys.release();
+    values.release();
+    sort_temp.release();
+    work_counter.release();
+  }
+};
+
 struct dpa_context {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -86,7 +100,7 @@ struct dpa_context {
   uint64_t staging_limit = 1ull << 30;
 
   DeviceBuffer positions, remaining, remaining_in, termination;
-  DeviceBuffer keys, values, sort_temp, work_counter;
+  dpa_launch_scratch scratch;
   uint64_t launches = 0;  // kernels this context launched (advection path)
   bool profiling = false;
   cudaEvent_t events[3] = {nullptr, nullptr, nullptr};  // order, advect begin, advect end
@@ -99,8 +113,9 @@ struct dpa_context {
   DeviceBuffer ftle_winners, ftle_flow, ftle_out, ftle_original, ftle_final;
 
   void release_all() {
-    DeviceBuffer* d[] = {&positions, &remaining, &remaining_in, &termination, &keys, &values,
-                         &sort_temp, &work_counter, &raw, &raw_offsets, &raw_counts,
+    scratch.release();
+    DeviceBuffer* d[] = {&positions, &remaining, &remaining_in, &termination, &raw, &raw_offsets,
+                         &raw_counts,
                          &kept_vertices, &kept_segments, &wide, &vertex_offsets,
                          &segment_offsets, &scan_temp, &totals, &out_vertices, &out_colors,
                          &out_indices, &ftle_winners, &ftle_flow, &ftle_out, &ftle_original,

@@ -250,7 +250,9 @@ int dpa_advect_batch_device(dpa_context* ctx, const dpa_field* field,
 /* The launch sequence of dpa_advect_device (processing order + advection) for
  * fixed device arrays, captured once into a CUDA graph; each
  * dpa_graph_launch replays it on a stream (NULL: the context's). The graph
- * shares the context's scratch: launch it on one stream at a time. */
+ * owns its scratch (8 bytes per particle and about 1 MB), so the context's
+ * other calls may run between replays; replays of one graph must not
+ * overlap. dpa_graph_destroy waits for the device. */
 int dpa_graph_create_advect(dpa_context* ctx, const dpa_field* field,
                             const dpa_advect_options* options, uint64_t count,
                             float* device_positions, uint64_t* device_remaining,

@@ -107,6 +107,40 @@ def test_graph_replay_matches_one_call(ctx, setup):
     ctx.check(ctx._lib.dpa_graph_destroy(ctx.handle, graph))
 
 
+def test_graph_replays_after_a_larger_call_on_its_context(ctx, setup):
+    # A graph keeps its own scratch: a call on the same context with four
+    # times the particles (which regrows the context's scratch) between two
+    # replays changes neither replay.
+    import torch
+    grid, field, p0, r0 = setup
+    want = reference_run(ctx, field, p0, r0)
+    pos, rem = p0.clone(), r0.clone()
+    term = torch.zeros(p0.shape[0], dtype=torch.uint8, device="cuda")
+    opts = N.AdvectOptions(N.INTEGRATORS["runge_kutta_4"], 0.25, 0, 0, 0, 1, 0)
+    graph = C.c_void_p()
+    ctx.check(ctx._lib.dpa_graph_create_advect(ctx.handle, field.handle, C.byref(opts),
+                                               p0.shape[0], _ptr(pos), _ptr(rem), _ptr(term),
+                                               C.byref(graph)))
+    big_want = None
+    for _ in range(2):
+        pos.copy_(p0)
+        rem.copy_(r0)
+        torch.cuda.synchronize()
+        ctx.check(ctx._lib.dpa_graph_launch(ctx.handle, graph, None))
+        ctx.synchronize()
+        np.testing.assert_array_equal(pos.cpu().numpy(), want[0])
+        np.testing.assert_array_equal(rem.cpu().numpy(), want[1])
+        np.testing.assert_array_equal(term.cpu().numpy(), want[2])
+        big = reference_run(ctx, field, p0.repeat(4, 1), r0.repeat(4))
+        if big_want is None:
+            big_want = big
+        for x, y in zip(big, big_want):
+            np.testing.assert_array_equal(x, y)
+    for x, y in zip(big_want, want):
+        np.testing.assert_array_equal(x, np.concatenate([y] * 4))
+    ctx.check(ctx._lib.dpa_graph_destroy(ctx.handle, graph))
+
+
 def test_autotune_keeps_results_identical(ctx, setup):
     grid, field, p0, r0 = setup
     want = reference_run(ctx, field, p0, r0)
