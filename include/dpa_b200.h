@@ -180,6 +180,9 @@ int dpa_field_create_device(dpa_context* ctx, const float* device_xyzv, const ui
                             const float offset[3], const float spacing[3], int32_t storage,
                             dpa_field** out);
 
+/* Waits for the context's stream, then frees the field. Graphs captured on a
+ * field and servers it was added to keep its device address: destroy them
+ * first. */
 int dpa_field_destroy(dpa_context* ctx, dpa_field* field);
 
 int dpa_field_info(const dpa_field* field, uint64_t shape[3], float offset[3], float spacing[3],
@@ -364,6 +367,8 @@ typedef struct dpa_server_stats {
 } dpa_server_stats;
 
 int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_server** out);
+/* Makes a field of the server's context resident for requests (at most 256
+ * fields); it must outlive the server. */
 int dpa_server_add_field(dpa_server* server, const dpa_field* field, int32_t* field_id);
 /* Queues a request; DPA_ERROR_OUT_OF_MEMORY when it could never fit the arenas. */
 int dpa_server_submit(dpa_server* server, const dpa_request* request, uint64_t* id);
