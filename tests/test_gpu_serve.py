@@ -3,7 +3,6 @@ concurrent requests (bit for bit), requests that do not fit wait for room,
 and requests that can never fit are refused. The mix holds requests of 4096
 seeds or more, which the server sweeps in the Morton order of their seeds,
 and smaller ones, swept in submission order."""
-import math
 import time
 
 import numpy as np

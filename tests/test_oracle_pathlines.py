@@ -3,7 +3,6 @@ counterpart in the reference): frozen slices reproduce the steady
 streamlines, the time axis follows the spatial rule, and a field linear in
 time matches a numpy restatement step by step."""
 import numpy as np
-import pytest
 
 from dpa_b200 import UnsteadyGrid, fields, seeds
 
