@@ -926,9 +926,13 @@ int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_adve
     DPA_TRY_CUDA(ctx, cudaMemcpyAsync(rem0.ptr, device_remaining, n * 8, cudaMemcpyDeviceToDevice, s));
     dpa_advect_options o = *options;
     if (sample_steps && (o.max_steps == 0 || sample_steps < o.max_steps)) o.max_steps = sample_steps;
-    cudaEvent_t e0, e1;
-    DPA_TRY_CUDA(ctx, cudaEventCreate(&e0));
-    DPA_TRY_CUDA(ctx, cudaEventCreate(&e1));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    const cudaError_t made = cudaEventCreate(&e0);
+    const cudaError_t made1 = made == cudaSuccess ? cudaEventCreate(&e1) : made;
+    if (made1 != cudaSuccess) {
+      if (e0) cudaEventDestroy(e0);
+      return fail_cuda(ctx, made1, "cudaEventCreate");
+    }
     const dpa_tuning_state saved = ctx->tuning;
     const bool profiling = ctx->profiling;
     ctx->profiling = false;

@@ -71,6 +71,9 @@ struct response_storage {
 struct dpa_server {
   dpa_context* ctx = nullptr;
   dpa_server_options options{};
+  // The context's launch tuning when the server was created: the worker
+  // reads it without the context, which other threads may retune.
+  dpa_tuning_state tuning;
   std::vector<const dpa_field*> fields;
   cudaStream_t stream = nullptr;
 
@@ -230,20 +233,20 @@ void dpa_server::upload(std::vector<active_request>& admitted, uint64_t first_ti
   SERVER_TRY(cudaStreamWaitEvent(stream, seeds_copied, 0));
   for (const active_request& a : admitted) {
     const uint64_t n = a.p.request.count;
-    if (n >= kServeOrderMin && ctx->tuning.order)
+    if (n >= kServeOrderMin && tuning.order)
       SERVER_TRY(dpa::launch_order(fields[size_t(a.p.request.field)]->view,
                                    positions.as<float>() + 3 * a.first, n,
                                    order_ids.as<uint32_t>() + a.first,
                                    order_counts.as<uint32_t>(),
                                    seed_order.as<uint32_t>() + a.first, stream,
-                                   ctx->tuning.order));
+                                   tuning.order));
   }
   for (const active_request& a : admitted) {
     const dpa_request& q = a.p.request;
     const uint64_t n = q.count;
     serve_init_kernel<<<unsigned(std::max<uint64_t>((n + 255) / 256, 1)), 256, 0, stream>>>(
         a.first, n, q.iterations, q.start_time, a.slot, q.record != 0, a.raw_first,
-        n >= kServeOrderMin && ctx->tuning.order, remaining.as<uint64_t>(),
+        n >= kServeOrderMin && tuning.order, remaining.as<uint64_t>(),
         remaining_initial.as<uint64_t>(), termination.as<uint8_t>(), request_of.as<uint32_t>(),
         times.as<float>(), raw_offsets.as<uint64_t>(), seed_order.as<uint32_t>(),
         in_flight.as<unsigned int>());
@@ -301,7 +304,7 @@ uint32_t dpa_server::tick(uint64_t steps, int parity) {
     a.termination = termination.as<uint8_t>();
     a.coefficients = dpa::make_step_coefficients(integrator, step_size);
     a.max_steps = steps;
-    a.claim = ctx->tuning.claim;
+    a.claim = tuning.claim;
     a.work_counter = work_counter.as<unsigned long long>();
     a.resume_only = true;
     a.request_of = request_of.as<uint32_t>();
@@ -608,6 +611,7 @@ int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_s
     auto s = std::make_unique<dpa_server>();
     s->ctx = ctx;
     s->options = *options;
+    s->tuning = ctx->tuning;
     if (cudaSetDevice(ctx->device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
       ctx->error = "server: cannot create a stream";

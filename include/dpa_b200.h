@@ -298,10 +298,11 @@ int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_adve
  * arrive while others run join at the next tick. A worker thread owns the
  * ticks; a second thread, on its own stream, copies out, emits and returns
  * the requests that have finished while the ticks go on. A request of 4096
- * seeds or more is swept in the Morton order of its seeds' start cells (the
- * context's tuning order; submission order when that is off). submit, poll
- * and stats may be called from any thread. The context is used for its
- * device, its fields and its tuning only. */
+ * seeds or more is swept in the Morton order of its seeds' start cells. The
+ * launches use the context's tuning (dpa_context_set_tuning) as it was when
+ * the server was created; an order of 0 there sweeps requests in submission
+ * order. submit, poll and stats may be called from any thread. The context is
+ * used for its device, its fields and that tuning only. */
 typedef struct dpa_server_options {
   uint64_t particle_capacity;  /* particle slots of the arena (62 bytes each) */
   uint64_t vertex_capacity;    /* curve-staging vertices of the arena (12 bytes each) */
