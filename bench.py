@@ -1104,6 +1104,13 @@ def run_secondary(a):
                             "is this end-to-end call"},
         })
         algorithmic = None
+        # Positions against the FP64 oracle integrator, every seed, at
+        # horizons most seeds still live to (half have left the domain by
+        # step 100, nearly all by step 500).
+        config = types.SimpleNamespace(integrator=a.integrator, step_size=step,
+                                       iterations=iterations)
+        out["fp64_error"] = fp64_error(config, ctx, field, grid, parts, sample=n,
+                                       horizons=(50, 100, 250))
         out["at_scale"] = recording_at_scale(ctx, a)
     launches1 = C.c_uint64()
     ctx.check(lib.dpa_context_launch_count(ctx.handle, C.byref(launches1)))
