@@ -20,6 +20,8 @@ STATUS_NAMES = {
     4: "DPA_ERROR_CUDA",
     5: "DPA_ERROR_SINK",
     6: "DPA_ERROR_INTERNAL",
+    7: "DPA_ERROR_TIMEOUT",
+    8: "DPA_ERROR_CANCELLED",
 }
 
 STORAGE = {"f32": 0, "f16": 1, "bf16": 2}
@@ -36,7 +38,8 @@ INTEGRATORS = {
     "runge_kutta_4_true": 100,
 }
 
-TERMINATION = {0: "complete", 1: "out_of_bounds", 2: "zero_velocity", 3: "in_flight"}
+TERMINATION = {0: "complete", 1: "out_of_bounds", 2: "zero_velocity", 3: "in_flight",
+               4: "cancelled"}
 
 FTLE_MAPPING = {"reference": 0, "lattice": 1}
 
@@ -74,6 +77,8 @@ class Tuning(C.Structure):
         ("blocks_per_sm", C.c_uint32),
         ("order", C.c_uint32),
         ("measured_ms", C.c_float),
+        ("block_size", C.c_uint32),
+        ("particles_per_thread", C.c_uint32),
     ]
 
 
@@ -83,6 +88,9 @@ class ServerOptions(C.Structure):
         ("vertex_capacity", C.c_uint64),
         ("steps_per_tick", C.c_uint32),
         ("max_requests", C.c_uint32),
+        ("small_request_seeds", C.c_uint64),
+        ("reserved_percent", C.c_uint32),
+        ("max_bypass_ms", C.c_uint32),
     ]
 
 
@@ -100,6 +108,7 @@ class Request(C.Structure):
         ("iterations", C.c_uint64),
         ("user", C.c_void_p),
         ("start_time", C.c_float),
+        ("deadline_ms", C.c_uint32),
     ]
 
 
@@ -160,7 +169,10 @@ SIGNATURES = {
     "dpa_context_set_staging_limit": (C.c_int, [_P, C.c_uint64]),
     "dpa_context_set_profiling": (C.c_int, [_P, C.c_int32]),
     "dpa_context_last_timing": (C.c_int, [_P, _F32P, _F32P]),
+    "dpa_context_last_emit_timing": (C.c_int, [_P, _F32P]),
     "dpa_context_launch_count": (C.c_int, [_P, _U64P]),
+    "dpa_measure_gather_bandwidth": (C.c_int, [_P, C.c_uint64, C.c_int32,
+                                               C.POINTER(C.c_double)]),
     "dpa_integrator_from_name": (C.c_int, [C.c_char_p, C.POINTER(C.c_int32)]),
     "dpa_field_create": (C.c_int, [_P, _P, _U64P, _F32P, _F32P, C.c_int32, C.POINTER(C.c_void_p)]),
     "dpa_field_create_device": (C.c_int, [_P, _P, _U64P, _F32P, _F32P, C.c_int32,
@@ -190,6 +202,7 @@ SIGNATURES = {
     "dpa_server_submit": (C.c_int, [_P, C.POINTER(Request), _U64P]),
     "dpa_server_poll": (C.c_int, [_P, C.c_int32, C.POINTER(Response), C.POINTER(C.c_int32)]),
     "dpa_server_release": (C.c_int, [_P, C.c_uint64]),
+    "dpa_server_cancel": (C.c_int, [_P, C.c_uint64]),
     "dpa_server_get_stats": (C.c_int, [_P, C.POINTER(ServerStats)]),
     "dpa_server_destroy": (C.c_int, [_P]),
     "dpa_advect_device_no_alloc": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _P, _P,

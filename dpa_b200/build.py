@@ -10,6 +10,7 @@ Outputs (git-ignored, shipped with the tree):
 """
 from __future__ import annotations
 
+import hashlib
 import os
 import shutil
 import subprocess
@@ -25,8 +26,8 @@ LIBRARY = PACKAGE / "libdpa_b200.so"
 PIPELINE = PACKAGE / "bin" / "dpa_pipeline"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SOURCES = ["capi.cu", "advect.cu", "advect_unsteady.cu", "emit.cu", "ftle.cu", "noalloc.cu",
-                "serve.cu"]
+CUDA_SOURCES = ["capi.cu", "advect.cu", "advect_f32.cu", "advect_f16.cu", "advect_bf16.cu",
+                "emit.cu", "ftle.cu", "noalloc.cu", "serve.cu"]
 
 
 def nvcc() -> str:
@@ -36,11 +37,30 @@ def nvcc() -> str:
     raise RuntimeError("nvcc not found")
 
 
-def _stale(target: Path, sources: list[Path]) -> bool:
-    if not target.exists():
+def _digest(sources: list[Path], command: list[str]) -> str:
+    """Hash of the sources' contents and of the build command."""
+    h = hashlib.sha256()
+    for s in sorted(sources):
+        h.update(str(s.relative_to(ROOT)).encode())
+        h.update(s.read_bytes())
+    # The tree may sit elsewhere on another machine: paths inside it count
+    # relative to its root.
+    h.update(" ".join(command).replace(str(ROOT), "<root>").encode())
+    return h.hexdigest()
+
+
+def _stale(target: Path, sources: list[Path], command: list[str]) -> bool:
+    """A target is rebuilt unless its stamp records the current sources and
+    command (content, not timestamps: a tree copied with newer modification
+    times than its sources still rebuilds when the sources changed)."""
+    stamp = target.with_name(target.name + ".stamp")
+    if not target.exists() or not stamp.exists():
         return True
-    t = target.stat().st_mtime
-    return any(s.stat().st_mtime > t for s in sources)
+    return stamp.read_text().strip() != _digest(sources, command)
+
+
+def _stamp(target: Path, sources: list[Path], command: list[str]) -> None:
+    target.with_name(target.name + ".stamp").write_text(_digest(sources, command) + "\n")
 
 
 def _run(cmd: list[str]) -> None:
@@ -48,25 +68,27 @@ def _run(cmd: list[str]) -> None:
     subprocess.run(cmd, check=True)
 
 
-def build_library(force: bool = False, verbose_ptxas: bool = False) -> Path:
+def build_library(force: bool = False, verbose_ptxas: bool = False,
+                  defines: tuple[str, ...] = ()) -> Path:
     sources = [CSRC / s for s in CUDA_SOURCES]
-    deps = sources + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.hpp")) + [INCLUDE / "dpa_b200.h"]
-    if not force and not _stale(LIBRARY, deps):
+    deps = sources + sorted(CSRC.glob("*.cuh")) + sorted(CSRC.glob("*.hpp")) + \
+        [INCLUDE / "dpa_b200.h"]
+    flags = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
+                    "-I", str(INCLUDE), "-I", str(CSRC), "--expt-relaxed-constexpr"]
+    flags += [f"-D{d}" for d in defines]
+    if not force and not _stale(LIBRARY, deps, flags):
         return LIBRARY
     build_dir = PACKAGE / "_build"
     build_dir.mkdir(exist_ok=True)
     objects = []
-    flags = ARCH + ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC",
-                    "-I", str(INCLUDE), "-I", str(CSRC), "--expt-relaxed-constexpr"]
-    if verbose_ptxas:
-        flags += ["-Xptxas", "-v"]
+    compile_flags = flags + (["-Xptxas", "-v"] if verbose_ptxas else [])
     # The translation units compile in parallel (the advection kernel's
-    # instantiations dominate and are split across two of them).
+    # instantiations dominate and are split by field storage).
     from concurrent.futures import ThreadPoolExecutor
     commands = []
     for src in sources:
         obj = build_dir / (src.stem + ".o")
-        commands.append([nvcc(), "-c", str(src), "-o", str(obj)] + flags)
+        commands.append([nvcc(), "-c", str(src), "-o", str(obj)] + compile_flags)
         objects.append(str(obj))
     with ThreadPoolExecutor(max_workers=min(len(commands), os.cpu_count() or 1)) as pool:
         for f in [pool.submit(_run, c) for c in commands]:
@@ -74,6 +96,7 @@ def build_library(force: bool = False, verbose_ptxas: bool = False) -> Path:
     tmp = LIBRARY.with_suffix(".so.tmp")
     _run([nvcc()] + ARCH + ["-shared", "-o", str(tmp)] + objects + ["-cudart", "static"])
     os.replace(tmp, LIBRARY)
+    _stamp(LIBRARY, deps, flags)
     return LIBRARY
 
 
@@ -93,18 +116,22 @@ def build_host(force: bool = False) -> Path:
     sources = [HOST / s for s in HOST_SOURCES]
     deps = sources + sorted(HOST.glob("*.hpp")) + sorted(HOST.glob("*.h")) + [
         INCLUDE / "dpa_b200.h", LIBRARY]
-    if force or _stale(HOST_LIBRARY, deps):
+    command = [host_compiler(), "-std=c++17", "-O2", "-Wall", "-fPIC", "-shared",
+               "-I", str(INCLUDE), "-I", str(HOST)] + [str(s) for s in sources]
+    if force or _stale(HOST_LIBRARY, deps, command):
         tmp = HOST_LIBRARY.with_suffix(".so.tmp")
-        _run([host_compiler(), "-std=c++17", "-O2", "-Wall", "-fPIC", "-shared",
-              "-I", str(INCLUDE), "-I", str(HOST)] + [str(s) for s in sources] +
-             ["-o", str(tmp), "-L", str(PACKAGE), "-ldpa_b200", "-Wl,-rpath,$ORIGIN"])
+        _run(command + ["-o", str(tmp), "-L", str(PACKAGE), "-ldpa_b200", "-Wl,-rpath,$ORIGIN"])
         os.replace(tmp, HOST_LIBRARY)
+        _stamp(HOST_LIBRARY, deps, command)
     main = HOST / "main.cpp"
-    if force or _stale(PIPELINE, [main, HOST_LIBRARY, HOST / "pipeline.hpp"]):
+    main_deps = [main, HOST_LIBRARY, HOST / "pipeline.hpp"]
+    main_command = [host_compiler(), "-std=c++17", "-O2", "-Wall", "-I", str(INCLUDE), "-I",
+                    str(HOST), str(main)]
+    if force or _stale(PIPELINE, main_deps, main_command):
         PIPELINE.parent.mkdir(exist_ok=True)
-        _run([host_compiler(), "-std=c++17", "-O2", "-Wall", "-I", str(INCLUDE), "-I", str(HOST),
-              str(main), "-o", str(PIPELINE), "-L", str(PACKAGE), "-ldpa_host", "-ldpa_b200",
-              "-Wl,-rpath,$ORIGIN/.."])
+        _run(main_command + ["-o", str(PIPELINE), "-L", str(PACKAGE), "-ldpa_host", "-ldpa_b200",
+                             "-Wl,-rpath,$ORIGIN/.."])
+        _stamp(PIPELINE, main_deps, main_command)
     return HOST_LIBRARY
 
 

@@ -1,8 +1,8 @@
-// advect.cu -- steady-field advection launches and the processing-order,
+// advect.cu -- the advection launch dispatch and the processing-order,
 // batch and serving helper kernels.
 #include <algorithm>
 
-#include "advect_kernel.cuh"
+#include "kernels.cuh"
 
 namespace dpa {
 
@@ -167,7 +167,84 @@ __global__ void expand_ranges_kernel(const uint64_t* starts, const uint64_t* fir
   list[t] = uint32_t(start + order[start + (t - firsts[lo])]);
 }
 
+// Counts the dividends a (every 32-bit pattern) for which
+// divide_by_reciprocal(a, h, y) and __fdiv_rn(a, h) differ in their bits.
+// Results that are both non-finite count as equal: either one places a
+// position outside the grid.
+__global__ void verify_division_kernel(float h, float y, unsigned int* mismatches) {
+  const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
+  unsigned int bad = 0;
+  for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < (1ull << 32);
+       i += stride) {
+    const float a = __uint_as_float(uint32_t(i));
+    const float want = __fdiv_rn(a, h);
+    const float got = divide_by_reciprocal(a, h, y);
+    const bool same = __float_as_uint(want) == __float_as_uint(got) ||
+                      (!isfinite(want) && !isfinite(got));
+    bad += same ? 0u : 1u;
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) bad += __shfl_down_sync(0xffffffffu, bad, o);
+  if ((threadIdx.x & 31u) == 0 && bad) atomicAdd(mismatches, bad);
+}
+
+// Data-path probe: every lane loads, per iteration, the eight 16-byte nodes
+// of one cell (four edges of two consecutive nodes, the advection kernel's
+// gather), from a table of mask + 1 nodes laid out as a cube of side 2^side.
+// Random: each lane's cell is drawn by xorshift32 (Marsaglia, "Xorshift
+// RNGs", 2003). Coalesced: the warp's lanes read consecutive cells, so each
+// load instruction covers four 128-byte lines (the data path's ceiling).
+__global__ void __launch_bounds__(256) gather_probe_kernel(const float4* table, uint32_t mask,
+                                                           uint32_t side, uint32_t iterations,
+                                                           int random, float* sink) {
+  const uint32_t s1 = 1u << side, s0 = 1u << (2 * side);
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  uint32_t x = (blockIdx.x * blockDim.x + threadIdx.x) * 2654435761u + 1u;
+  uint32_t cursor = warp * 64u;
+  // Random: the second node of an edge follows the first; coalesced: the
+  // warp's first loads cover 32 consecutive nodes and its second loads the
+  // next 32.
+  const uint32_t pair = random ? 1u : 32u;
+  float acc = 0.0f;
+  for (uint32_t i = 0; i < iterations; ++i) {
+    uint32_t c;
+    if (random) {
+      x ^= x << 13;
+      x ^= x >> 17;
+      x ^= x << 5;
+      c = x;
+    } else {
+      c = cursor + lane;
+      cursor += 64u * warps;
+    }
+    const uint32_t e[4] = {c, c + s1, c + s0, c + s0 + s1};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float4 a = __ldg(table + (e[k] & mask));
+      const float4 b = __ldg(table + ((e[k] + pair) & mask));
+      acc += a.x + a.y + a.z + b.x + b.y + b.z;
+    }
+  }
+  if (acc == 1.5f) *sink = acc;  // keeps the loads; the table holds no such sum
+}
+
 }  // namespace
+
+cudaError_t launch_gather_probe(const float4* table, uint32_t mask, uint32_t side,
+                                uint32_t iterations, int random, float* sink, uint32_t blocks,
+                                cudaStream_t stream) {
+  gather_probe_kernel<<<blocks, 256, 0, stream>>>(table, mask, side, iterations, random, sink);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_verify_division(float h, float y, unsigned int* mismatches,
+                                   cudaStream_t stream) {
+  DPA_CUDA_TRY(cudaMemsetAsync(mismatches, 0, sizeof(unsigned int), stream));
+  verify_division_kernel<<<148 * 8, 256, 0, stream>>>(h, y, mismatches);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_expand_ranges(const uint64_t* starts, const uint64_t* firsts, uint32_t ranges,
                                  uint64_t total, const uint32_t* order, uint32_t* list,
@@ -188,12 +265,25 @@ cudaError_t launch_set_steps(const uint64_t* remaining_in, const uint64_t* remai
 
 cudaError_t launch_advect(const FieldView& f, const AdvectArgs& a, int integrator, bool record,
                           cudaStream_t stream) {
-  if (f.slices > 1) return launch_advect_unsteady(f, a, integrator, record, stream);
-  return launch_family<false>(f, a, integrator, record, stream);
+  const bool unsteady = f.slices > 1;
+  switch (f.storage) {
+    case DPA_STORAGE_F32:
+      return unsteady ? launch_advect_storage<DPA_STORAGE_F32, true>(f, a, integrator, record, stream)
+                      : launch_advect_storage<DPA_STORAGE_F32, false>(f, a, integrator, record, stream);
+    case DPA_STORAGE_F16:
+      return unsteady ? launch_advect_storage<DPA_STORAGE_F16, true>(f, a, integrator, record, stream)
+                      : launch_advect_storage<DPA_STORAGE_F16, false>(f, a, integrator, record, stream);
+    case DPA_STORAGE_BF16:
+      return unsteady ? launch_advect_storage<DPA_STORAGE_BF16, true>(f, a, integrator, record, stream)
+                      : launch_advect_storage<DPA_STORAGE_BF16, false>(f, a, integrator, record, stream);
+    default:
+      return cudaErrorInvalidValue;
+  }
 }
 
-cudaError_t prepare_advect(const FieldView& f, int integrator, bool record) {
-  AdvectArgs a{};
+cudaError_t prepare_advect(const FieldView& f, const AdvectArgs& launch, int integrator,
+                           bool record) {
+  AdvectArgs a = launch;
   a.count = 0;
   return launch_advect(f, a, integrator, record, nullptr);
 }

@@ -1,0 +1,10 @@
+// advect_bf16.cu -- the advection kernels of BF16 fields, steady and time-varying
+// (a compile split: each storage's instantiations build in parallel).
+#include "advect_kernel.cuh"
+
+namespace dpa {
+template cudaError_t launch_advect_storage<DPA_STORAGE_BF16, false>(const FieldView&, const AdvectArgs&,
+                                                                   int, bool, cudaStream_t);
+template cudaError_t launch_advect_storage<DPA_STORAGE_BF16, true>(const FieldView&, const AdvectArgs&,
+                                                                  int, bool, cudaStream_t);
+}  // namespace dpa

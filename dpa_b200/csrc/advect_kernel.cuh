@@ -1,10 +1,11 @@
 // advect_kernel.cuh -- the advection kernel template and its launchers:
-// one thread per particle, every step of that particle in registers
-// (particle_advector.cpp:325-396). advect.cu instantiates it for steady
-// fields, advect_unsteady.cu for time-varying ones.
+// every step of a particle in registers (particle_advector.cpp:325-396), one
+// or two particles per lane. advect_f32.cu, advect_f16.cu and advect_bf16.cu
+// instantiate it per field storage, for steady and time-varying fields.
 #pragma once
 
 #include <algorithm>
+#include <atomic>
 #include <type_traits>
 
 #include "kernels.cuh"
@@ -31,263 +32,343 @@ struct CurveCounter {
   }
 };
 
-// Persistent advection: every lane owns one particle at a time and, when it
-// finishes, takes the next one from its warp's claim of a.claim consecutive
-// entries of the processing order; the warp claims a new batch with one
-// atomic when its batch runs out. Lanes therefore stay busy while particles
-// of one warp end after very different numbers of steps. A particle takes at
-// most a.max_steps steps per launch; one stopped by that budget alone is
-// reported as in flight and resumes in a later launch.
+template <int kIntegrator, bool kUnsteady, int kPPT>
+constexpr int advect_min_blocks() {
+  return kPPT == 2                                       ? kAdvectPpt2MinBlocks
+         : kUnsteady                                     ? kAdvectUnsteadyMinBlocks
+         : kIntegrator == DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE ? kAdvectTrueRk4MinBlocks
+                                                         : kAdvectMinBlocks;
+}
+
+// Persistent advection. Every lane owns kPPT slots, each holding one particle
+// at a time; a slot whose particle finishes takes the next one from its
+// warp's claim of a.claim consecutive entries of the processing order, and
+// the warp claims a new batch with one atomic when its batch runs out. Lanes
+// therefore stay busy while particles of one warp end after very different
+// numbers of steps. A particle takes at most a.max_steps steps per launch;
+// one stopped by that budget alone is reported as in flight and resumes in a
+// later launch.
 //
-// Between hand-outs the warp runs stretches: every active lane steps until
-// one of the warp's particles stops, with one vote per step and a 32-bit step
-// counter per stretch (a stretch ends at 2^32 - 1 steps at the latest).
-template <int kIntegrator, int kStorage, bool kPow2, bool kRecord, bool kUnsteady>
-__global__ void __launch_bounds__(kAdvectBlock,
-                                  kUnsteady ? kAdvectUnsteadyMinBlocks
-                                  : kIntegrator == DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE
-                                      ? kAdvectTrueRk4MinBlocks
-                                      : kAdvectMinBlocks)
+// Between hand-outs the warp runs stretches: every slot steps until one of
+// the warp's particles stops, with one vote per step and a 32-bit step
+// counter per stretch (a stretch ends at 2^32 - 1 steps at the latest). The
+// kPPT slots of a lane step in lock-step, so one particle's corner gather is
+// in flight while the other's arithmetic issues. An empty slot holds a NaN
+// position: its step fails the grid test at once, touches no memory and is
+// never counted.
+template <int kIntegrator, int kStorage, int kLocate, bool kRecord, bool kUnsteady, int kPPT>
+__global__ void __launch_bounds__(kAdvectBlock, advect_min_blocks<kIntegrator, kUnsteady, kPPT>())
 advect_kernel(const FieldView f, const AdvectArgs a) {
-  using Sampler = std::conditional_t<kUnsteady, TimeSampler<kStorage, kPow2>,
-                                     CellSampler<kStorage, kPow2>>;
+  using Sampler = std::conditional_t<kUnsteady, TimeSampler<kStorage, kLocate>,
+                                     CellSampler<kStorage, kLocate>>;
   constexpr unsigned kFull = 0xffffffffu;
   // State touched only when particles are handed out or finish lives in
   // shared memory, leaving the registers to the stepping loop: the warp's
-  // claim [next, end) of the order, and each lane's particle index.
+  // claim [next, end) of the order and, per slot, the particle index, its
+  // remaining iterations and the steps it may still take in this launch
+  // (its remaining iterations or the launch's step budget).
   __shared__ uint64_t claims[kAdvectBlock / 32][2];
-  __shared__ uint64_t particle[kAdvectBlock];
+  __shared__ uint64_t particle[kPPT][kAdvectBlock];
+  __shared__ uint64_t remaining[kPPT][kAdvectBlock];
+  __shared__ uint64_t budget[kPPT][kAdvectBlock];
   const uint32_t claim = a.claim;
-  const unsigned lane = threadIdx.x & 31u;
-  uint64_t* const warp_claim = claims[threadIdx.x >> 5];
+  const unsigned tid = threadIdx.x;
+  const unsigned lane = tid & 31u;
+  uint64_t* const warp_claim = claims[tid >> 5];
   if (lane == 0) warp_claim[0] = warp_claim[1] = 0;
   __syncwarp();
   bool exhausted = false;
+  const float nan = __int_as_float(0x7fffffff);
 
-  bool active = false;
-  // rem: the particle's remaining iterations; left: steps it may still take
-  // in this launch (its remaining iterations or the launch's step budget).
-  uint64_t rem = 0, left = 0;
-  Position p{0.0f, make_float2(0.0f, 0.0f)};
-  float* curve = nullptr;  // the particle's last written vertex
-  CurveCounter counter;
-  Sampler sampler;
-  StepHistory history{};
-  float t = 0.0f;  // particle time (a.times)
+  bool active[kPPT];
+  Position p[kPPT];
+  Sampler sampler[kPPT];
+  StepHistory history[kPPT];
+  float t[kPPT];          // particle time (a.times)
+  float* curve[kPPT];     // the particle's last written vertex
+  CurveCounter counter[kPPT];
+#pragma unroll
+  for (int j = 0; j < kPPT; ++j) {
+    active[j] = false;
+    p[j] = Position{nan, make_float2(nan, nan)};
+    history[j] = StepHistory{};
+    t[j] = 0.0f;
+    curve[j] = nullptr;
+  }
 
   while (true) {
-    // Hand new particles to idle lanes.
-    unsigned idle = __ballot_sync(kFull, !active);
-    while (idle && !exhausted) {
-      uint64_t next = warp_claim[0], end = warp_claim[1];
-      if (next == end) {
-        unsigned long long base = 0;
-        if (lane == 0) base = atomicAdd(a.work_counter, (unsigned long long)claim);
-        base = __shfl_sync(kFull, base, 0);
-        if (base >= a.count) {
-          exhausted = true;
-          break;
+    // Hand new particles to idle slots.
+#pragma unroll
+    for (int j = 0; j < kPPT; ++j) {
+      unsigned idle = __ballot_sync(kFull, !active[j]);
+      while (idle && !exhausted) {
+        uint64_t next = warp_claim[0], end = warp_claim[1];
+        if (next == end) {
+          unsigned long long base = 0;
+          if (lane == 0) base = atomicAdd(a.work_counter, (unsigned long long)claim);
+          base = __shfl_sync(kFull, base, 0);
+          if (base >= a.count) {
+            exhausted = true;
+            break;
+          }
+          next = base;
+          end = base + claim < a.count ? base + claim : a.count;
         }
-        next = base;
-        end = base + claim < a.count ? base + claim : a.count;
-      }
-      const uint32_t avail = uint32_t(end - next);
-      const uint32_t take = uint32_t(__popc(idle)) < avail ? uint32_t(__popc(idle)) : avail;
-      const uint32_t rank = __popc(idle & ((1u << lane) - 1u));
-      // Lanes still in the idle set take entries next + rank. (A lane that
-      // drew a finished particle earlier in this round is inactive but no
-      // longer idle, and must not take one again.)
-      const bool took = ((idle >> lane) & 1u) && rank < take;
-      bool mine = took;
-      uint64_t k = 0;
-      if (mine) {
-        const uint64_t e = next + rank;
-        k = a.order ? a.order[e] : e;
-        // Serving: a finished particle stays finished.
-        if (a.resume_only && a.termination[k] != DPA_TERMINATION_IN_FLIGHT) mine = false;
-      }
-      if (mine) {
-        particle[threadIdx.x] = k;
-        p.p0 = a.positions[3 * k];
-        p.p21 = make_float2(a.positions[3 * k + 2], a.positions[3 * k + 1]);
-        rem = a.remaining[k];
-        if (a.times) t = a.times[k];
-        left = rem < a.max_steps ? rem : a.max_steps;
-        sampler.reset();
-        history.started = false;
-        active = true;
-        if constexpr (kRecord) {
-          // A particle resumed from an earlier launch continues its curve
-          // where that launch left it.
-          const uint64_t done = a.remaining_initial ? a.remaining_initial[k] - rem : 0;
-          curve = a.raw_vertices + 3 * (a.raw_offsets[k] + done);
-          counter = CurveCounter();
-          if (done == 0) {
-            curve[0] = p.p0;
-            curve[1] = p.p21.y;
-            curve[2] = p.p21.x;
-            counter.append(p.p0, p.p21.y, p.p21.x);
-          } else {
-            counter.kept = a.kept_vertices[k];
-            counter.segments = a.kept_segments[k];
-            counter.prev_open = a.curve_open[k] != 0;
+        const uint32_t avail = uint32_t(end - next);
+        const uint32_t take = uint32_t(__popc(idle)) < avail ? uint32_t(__popc(idle)) : avail;
+        const uint32_t rank = __popc(idle & ((1u << lane) - 1u));
+        // Lanes still in the idle set take entries next + rank. (A slot that
+        // drew a finished particle earlier in this round is inactive but no
+        // longer idle, and must not take one again.)
+        const bool took = ((idle >> lane) & 1u) && rank < take;
+        bool mine = took;
+        uint64_t k = 0;
+        if (mine) {
+          const uint64_t e = next + rank;
+          k = a.order ? a.order[e] : e;
+          // Serving: a finished particle stays finished.
+          if (a.resume_only && a.termination[k] != DPA_TERMINATION_IN_FLIGHT) mine = false;
+        }
+        if (mine) {
+          particle[j][tid] = k;
+          p[j].p0 = a.positions[3 * k];
+          p[j].p21 = make_float2(a.positions[3 * k + 2], a.positions[3 * k + 1]);
+          const uint64_t rem = a.remaining[k];
+          remaining[j][tid] = rem;
+          budget[j][tid] = rem < a.max_steps ? rem : a.max_steps;
+          if (a.times) t[j] = a.times[k];
+          sampler[j].reset();
+          history[j].started = false;
+          active[j] = true;
+          if constexpr (kRecord) {
+            // A particle resumed from an earlier launch continues its curve
+            // where that launch left it.
+            const uint64_t done = a.remaining_initial ? a.remaining_initial[k] - rem : 0;
+            curve[j] = a.raw_vertices + 3 * (a.raw_offsets[k] + done);
+            counter[j] = CurveCounter();
+            if (done == 0) {
+              curve[j][0] = p[j].p0;
+              curve[j][1] = p[j].p21.y;
+              curve[j][2] = p[j].p21.x;
+              counter[j].append(p[j].p0, p[j].p21.y, p[j].p21.x);
+            } else {
+              counter[j].kept = a.kept_vertices[k];
+              counter[j].segments = a.kept_segments[k];
+              counter[j].prev_open = a.curve_open[k] != 0;
+            }
           }
         }
+        __syncwarp();
+        if (lane == 0) {
+          warp_claim[0] = next + take;
+          warp_claim[1] = end;
+        }
+        __syncwarp();
+        // Every lane that took an entry leaves this round of hand-outs; one
+        // that drew a finished particle (serving) stays inactive until the next.
+        idle &= ~__ballot_sync(kFull, took);
       }
-      __syncwarp();
-      if (lane == 0) {
-        warp_claim[0] = next + take;
-        warp_claim[1] = end;
-      }
-      __syncwarp();
-      // Every lane that took an entry leaves this round of hand-outs; one that
-      // drew a finished particle (serving) stays inactive until the next.
-      idle &= ~__ballot_sync(kFull, took);
     }
-    if (!__any_sync(kFull, active)) {
+    bool any = false;
+#pragma unroll
+    for (int j = 0; j < kPPT; ++j) any = any || active[j];
+    if (!__any_sync(kFull, any)) {
       if (exhausted) break;
       continue;  // every lane drew a finished particle (serving): claim again
     }
 
-    // One stretch. Inactive lanes (the order ran out) only vote.
-    const uint64_t allowed = active ? left : 0;
-    const uint32_t limit = allowed < 0xffffffffull ? uint32_t(allowed) : 0xffffffffu;
-    uint32_t it = 0;
-    int r = kStepTaken;
-    bool stop = active && limit == 0;
-    while (!__any_sync(kFull, stop)) {
-      if (active) {
-        r = step<kIntegrator>(f, a.coefficients, sampler, p, t, history);
-        if (r == kStepTaken) {
-          ++it;
-          if constexpr (kUnsteady) t = __fadd_rn(t, a.coefficients.dt);
+    // One stretch.
+    uint32_t it[kPPT], limit[kPPT];
+    int r[kPPT];
+    bool stop[kPPT];
+    bool halt = false;
+#pragma unroll
+    for (int j = 0; j < kPPT; ++j) {
+      const uint64_t allowed = active[j] ? budget[j][tid] : 0;
+      limit[j] = allowed < 0xffffffffull ? uint32_t(allowed) : 0xffffffffu;
+      it[j] = 0;
+      r[j] = kStepTaken;
+      stop[j] = active[j] && limit[j] == 0;
+      halt = halt || stop[j];
+    }
+    while (!__any_sync(kFull, halt)) {
+#pragma unroll
+      for (int j = 0; j < kPPT; ++j)
+        r[j] = step<kIntegrator>(f, a.coefficients, sampler[j], p[j], t[j], history[j]);
+      halt = false;
+#pragma unroll
+      for (int j = 0; j < kPPT; ++j) {
+        if (r[j] == kStepTaken) {  // never for an empty slot
+          ++it[j];
+          if constexpr (kUnsteady) t[j] = __fadd_rn(t[j], a.coefficients.dt);
           if constexpr (kRecord) {
-            float* v = curve + 3 * uint64_t(it);
-            v[0] = p.p0;
-            v[1] = p.p21.y;
-            v[2] = p.p21.x;
-            counter.append(p.p0, p.p21.y, p.p21.x);
+            float* v = curve[j] + 3 * uint64_t(it[j]);
+            v[0] = p[j].p0;
+            v[1] = p[j].p21.y;
+            v[2] = p[j].p21.x;
+            counter[j].append(p[j].p0, p[j].p21.y, p[j].p21.x);
           }
-          stop = it >= limit;
+          stop[j] = it[j] >= limit[j];
         } else {
-          stop = true;
+          stop[j] = true;
         }
+        halt = halt || (active[j] && stop[j]);
       }
     }
-    if (!active) continue;
-    rem -= it;
-    left -= it;
-    if constexpr (!kUnsteady) {
-      // A steady field's particles carry their time only when asked to; it
-      // advances by dt per step taken, rounded step by step as a
-      // time-varying field's does.
-      if (a.times)
-        for (uint32_t i = 0; i < it; ++i) t = __fadd_rn(t, a.coefficients.dt);
-    }
-    if constexpr (kRecord) curve += 3 * uint64_t(it);
-    // A particle that only reached the end of a stretch carries on.
-    if (!stop || (r == kStepTaken && left > 0)) continue;
 
-    const uint64_t k = particle[threadIdx.x];
-    const int reason = r == kStepOutOfBounds    ? DPA_TERMINATION_OUT_OF_BOUNDS
-                       : r == kStepZeroVelocity ? DPA_TERMINATION_ZERO_VELOCITY
-                       : rem == 0               ? DPA_TERMINATION_COMPLETE
-                                                : DPA_TERMINATION_IN_FLIGHT;
-    if constexpr (kRecord) {
-      if (reason != DPA_TERMINATION_IN_FLIGHT) {
-        float* v = curve + 3;
-        v[0] = kTerminal;
-        v[1] = kTerminal;
-        v[2] = kTerminal;
-        counter.append(kTerminal, kTerminal, kTerminal);
-      } else {
-        a.curve_open[k] = counter.prev_open ? 1 : 0;
+#pragma unroll
+    for (int j = 0; j < kPPT; ++j) {
+      if (!active[j]) continue;
+      const uint64_t rem = remaining[j][tid] - it[j];
+      const uint64_t left = budget[j][tid] - it[j];
+      remaining[j][tid] = rem;
+      budget[j][tid] = left;
+      if constexpr (!kUnsteady) {
+        // A steady field's particles carry their time only when asked to; it
+        // advances by dt per step taken, rounded step by step as a
+        // time-varying field's does.
+        if (a.times)
+          for (uint32_t i = 0; i < it[j]; ++i) t[j] = __fadd_rn(t[j], a.coefficients.dt);
       }
-      a.kept_vertices[k] = counter.kept;
-      a.kept_segments[k] = counter.segments;
+      if constexpr (kRecord) curve[j] += 3 * uint64_t(it[j]);
+      // A particle that only reached the end of a stretch carries on.
+      if (!stop[j] || (r[j] == kStepTaken && left > 0)) continue;
+
+      const uint64_t k = particle[j][tid];
+      const int reason = r[j] == kStepOutOfBounds    ? DPA_TERMINATION_OUT_OF_BOUNDS
+                         : r[j] == kStepZeroVelocity ? DPA_TERMINATION_ZERO_VELOCITY
+                         : rem == 0                  ? DPA_TERMINATION_COMPLETE
+                                                     : DPA_TERMINATION_IN_FLIGHT;
+      if constexpr (kRecord) {
+        if (reason != DPA_TERMINATION_IN_FLIGHT) {
+          float* v = curve[j] + 3;
+          v[0] = kTerminal;
+          v[1] = kTerminal;
+          v[2] = kTerminal;
+          counter[j].append(kTerminal, kTerminal, kTerminal);
+        } else {
+          a.curve_open[k] = counter[j].prev_open ? 1 : 0;
+        }
+        a.kept_vertices[k] = counter[j].kept;
+        a.kept_segments[k] = counter[j].segments;
+      }
+      a.positions[3 * k] = p[j].p0;
+      a.positions[3 * k + 1] = p[j].p21.y;
+      a.positions[3 * k + 2] = p[j].p21.x;
+      a.remaining[k] = rem;
+      if (a.times) a.times[k] = t[j];
+      if (a.termination) a.termination[k] = uint8_t(reason);
+      if (a.in_flight && reason != DPA_TERMINATION_IN_FLIGHT)
+        atomicSub(a.in_flight + a.request_of[k], 1u);
+      active[j] = false;
+      p[j] = Position{nan, make_float2(nan, nan)};
     }
-    a.positions[3 * k] = p.p0;
-    a.positions[3 * k + 1] = p.p21.y;
-    a.positions[3 * k + 2] = p.p21.x;
-    a.remaining[k] = rem;
-    if (a.times) a.times[k] = t;
-    if (a.termination) a.termination[k] = uint8_t(reason);
-    if (a.in_flight && reason != DPA_TERMINATION_IN_FLIGHT)
-      atomicSub(a.in_flight + a.request_of[k], 1u);
-    active = false;
   }
 }
 
-template <int kIntegrator, int kStorage, bool kPow2, bool kRecord, bool kUnsteady>
-cudaError_t resident_blocks(int* blocks_per_sm, int* sms) {
-  // Per instantiation and process; every device of a process is a B200 here.
-  static int resident = 0;
-  static int count = 0;
-  if (resident == 0) {
-    int device = 0;
+// Resident blocks per SM of one instantiation at one block size, and the SM
+// count, looked up once per process (every device of a process is a B200
+// here) and published as one atomic value, so that threads making their
+// first launches at once each see either nothing or both figures.
+template <int kIntegrator, int kStorage, int kLocate, bool kRecord, bool kUnsteady, int kPPT>
+cudaError_t resident_blocks(uint32_t block, int* blocks_per_sm, int* sms) {
+  static std::atomic<uint64_t> cache[kAdvectBlock / 32 + 1] = {};
+  std::atomic<uint64_t>& slot = cache[block / 32];
+  uint64_t packed = slot.load(std::memory_order_acquire);
+  if (packed == 0) {
+    int device = 0, count = 0, r = 0;
     DPA_CUDA_TRY(cudaGetDevice(&device));
     DPA_CUDA_TRY(cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, device));
-    int r = 0;
     DPA_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &r, advect_kernel<kIntegrator, kStorage, kPow2, kRecord, kUnsteady>, kAdvectBlock, 0));
-    resident = r < 1 ? 1 : r;
+        &r, advect_kernel<kIntegrator, kStorage, kLocate, kRecord, kUnsteady, kPPT>, int(block),
+        0));
+    packed = (uint64_t(uint32_t(count)) << 32) | uint32_t(r < 1 ? 1 : r);
+    slot.store(packed, std::memory_order_release);
   }
-  *blocks_per_sm = resident;
-  *sms = count;
+  *blocks_per_sm = int(uint32_t(packed));
+  *sms = int(packed >> 32);
   return cudaSuccess;
 }
 
-template <int kIntegrator, int kStorage, bool kPow2, bool kRecord, bool kUnsteady>
+// Threads per block of a launch: the tuning's choice, else kAdvectBlock, or
+// fewer (a multiple of 32) when the particles would fill fewer blocks than
+// the device has SMs, so that a small launch still spreads over every SM.
+inline uint32_t advect_block(const AdvectArgs& a, uint64_t lanes, int sms) {
+  if (a.block) return a.block;
+  uint32_t block = uint32_t(kAdvectBlock);
+#if DPA_ADVECT_SPREAD
+  const uint64_t per_sm = (lanes + uint64_t(sms) - 1) / uint64_t(sms);
+  if (per_sm < uint64_t(kAdvectBlock)) block = uint32_t(std::max<uint64_t>(32, (per_sm + 31) / 32 * 32));
+#else
+  (void)lanes;
+  (void)sms;
+#endif
+  return block;
+}
+
+template <int kIntegrator, int kStorage, int kLocate, bool kRecord, bool kUnsteady, int kPPT>
 cudaError_t launch_typed(const FieldView& f, const AdvectArgs& a, cudaStream_t stream) {
   // Persistent grid: as many blocks as fit on the device at once (or as the
   // tuning asks), fewer when there are fewer particles than lanes.
-  int resident = 0, sms = 0;
-  DPA_CUDA_TRY((resident_blocks<kIntegrator, kStorage, kPow2, kRecord, kUnsteady>(&resident, &sms)));
+  const uint64_t lanes = (a.count + kPPT - 1) / kPPT;
+  int sms = 0, resident = 0;
+  DPA_CUDA_TRY((resident_blocks<kIntegrator, kStorage, kLocate, kRecord, kUnsteady, kPPT>(
+      kAdvectBlock, &resident, &sms)));
+  const uint32_t block = advect_block(a, lanes, sms);
+  if (block == 0 || block % 32 != 0 || block > uint32_t(kAdvectBlock)) return cudaErrorInvalidValue;
+  DPA_CUDA_TRY((resident_blocks<kIntegrator, kStorage, kLocate, kRecord, kUnsteady, kPPT>(
+      block, &resident, &sms)));
   if (a.count == 0) return cudaSuccess;  // nothing to do, or preparation only
   if (a.blocks_per_sm && int(a.blocks_per_sm) < resident) resident = int(a.blocks_per_sm);
-  const uint64_t needed = (a.count + kAdvectBlock - 1) / kAdvectBlock;
+  const uint64_t needed = (lanes + block - 1) / block;
   const uint64_t blocks = std::min<uint64_t>(needed, uint64_t(resident) * uint64_t(sms));
   if (blocks == 0) return cudaSuccess;
   DPA_CUDA_TRY(cudaMemsetAsync(a.work_counter, 0, sizeof(unsigned long long), stream));
-  advect_kernel<kIntegrator, kStorage, kPow2, kRecord, kUnsteady>
-      <<<dim3(unsigned(blocks)), dim3(kAdvectBlock), 0, stream>>>(f, a);
+  advect_kernel<kIntegrator, kStorage, kLocate, kRecord, kUnsteady, kPPT>
+      <<<dim3(unsigned(blocks)), dim3(block), 0, stream>>>(f, a);
   return cudaGetLastError();
 }
 
+// Two particles per lane for steady fields without recording; everything
+// else runs one.
+template <int kIntegrator, int kStorage, int kLocate, bool kRecord, bool kUnsteady>
+cudaError_t launch_ppt(const FieldView& f, const AdvectArgs& a, cudaStream_t s) {
+  if constexpr (!kRecord && !kUnsteady && kIntegrator != DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE) {
+    if (a.particles_per_thread == 2)
+      return launch_typed<kIntegrator, kStorage, kLocate, kRecord, kUnsteady, 2>(f, a, s);
+  }
+  return launch_typed<kIntegrator, kStorage, kLocate, kRecord, kUnsteady, 1>(f, a, s);
+}
+
 template <int kIntegrator, int kStorage, bool kUnsteady>
-cudaError_t launch_pow2(const FieldView& f, const AdvectArgs& a, bool record, cudaStream_t s) {
-  if (f.pow2) {
-    return record ? launch_typed<kIntegrator, kStorage, true, true, kUnsteady>(f, a, s)
-                  : launch_typed<kIntegrator, kStorage, true, false, kUnsteady>(f, a, s);
-  }
-  return record ? launch_typed<kIntegrator, kStorage, false, true, kUnsteady>(f, a, s)
-                : launch_typed<kIntegrator, kStorage, false, false, kUnsteady>(f, a, s);
-}
-
-template <int kIntegrator, bool kUnsteady>
-cudaError_t launch_storage(const FieldView& f, const AdvectArgs& a, bool record, cudaStream_t s) {
-  switch (f.storage) {
-    case DPA_STORAGE_F32:
-      return launch_pow2<kIntegrator, DPA_STORAGE_F32, kUnsteady>(f, a, record, s);
-    case DPA_STORAGE_F16:
-      return launch_pow2<kIntegrator, DPA_STORAGE_F16, kUnsteady>(f, a, record, s);
-    case DPA_STORAGE_BF16:
-      return launch_pow2<kIntegrator, DPA_STORAGE_BF16, kUnsteady>(f, a, record, s);
-    default: return cudaErrorInvalidValue;
+cudaError_t launch_locate(const FieldView& f, const AdvectArgs& a, bool record, cudaStream_t s) {
+  switch (f.locate) {
+    case kLocatePow2:
+      return record ? launch_ppt<kIntegrator, kStorage, kLocatePow2, true, kUnsteady>(f, a, s)
+                    : launch_ppt<kIntegrator, kStorage, kLocatePow2, false, kUnsteady>(f, a, s);
+    case kLocateReciprocal:
+      return record ? launch_ppt<kIntegrator, kStorage, kLocateReciprocal, true, kUnsteady>(f, a, s)
+                    : launch_ppt<kIntegrator, kStorage, kLocateReciprocal, false, kUnsteady>(f, a, s);
+    default:
+      return record ? launch_ppt<kIntegrator, kStorage, kLocateDivide, true, kUnsteady>(f, a, s)
+                    : launch_ppt<kIntegrator, kStorage, kLocateDivide, false, kUnsteady>(f, a, s);
   }
 }
 
-// Every integrator for one kind of field (steady or time-varying).
-template <bool kUnsteady>
-cudaError_t launch_family(const FieldView& f, const AdvectArgs& a, int integrator, bool record,
-                          cudaStream_t stream) {
+}  // namespace
+
+// Every integrator for one storage and kind of field (steady or time-varying).
+template <int kStorage, bool kUnsteady>
+cudaError_t launch_advect_storage(const FieldView& f, const AdvectArgs& a, int integrator,
+                                  bool record, cudaStream_t stream) {
   switch (integrator) {
     case DPA_INTEGRATOR_EULER:
-      return launch_storage<DPA_INTEGRATOR_EULER, kUnsteady>(f, a, record, stream);
+      return launch_locate<DPA_INTEGRATOR_EULER, kStorage, kUnsteady>(f, a, record, stream);
     case DPA_INTEGRATOR_RUNGE_KUTTA_4:
-      return launch_storage<DPA_INTEGRATOR_RUNGE_KUTTA_4, kUnsteady>(f, a, record, stream);
+      return launch_locate<DPA_INTEGRATOR_RUNGE_KUTTA_4, kStorage, kUnsteady>(f, a, record, stream);
     case DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE:
-      return launch_storage<DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE, kUnsteady>(f, a, record, stream);
+      return launch_locate<DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE, kStorage, kUnsteady>(f, a, record,
+                                                                                  stream);
     case DPA_INTEGRATOR_MODIFIED_MIDPOINT:
     case DPA_INTEGRATOR_RUNGE_KUTTA_CASH_KARP_54:
     case DPA_INTEGRATOR_RUNGE_KUTTA_DORMAND_PRINCE_5:
@@ -295,11 +376,10 @@ cudaError_t launch_family(const FieldView& f, const AdvectArgs& a, int integrato
     case DPA_INTEGRATOR_ADAMS_BASHFORTH_2:
     case DPA_INTEGRATOR_ADAMS_BASHFORTH_MOULTON_2:
       // The coefficients in a.coefficients.g select the stepper.
-      return launch_storage<kGeneralIntegrator, kUnsteady>(f, a, record, stream);
+      return launch_locate<kGeneralIntegrator, kStorage, kUnsteady>(f, a, record, stream);
     default:
       return cudaErrorInvalidValue;
   }
 }
 
-}  // namespace
 }  // namespace dpa

@@ -3,16 +3,17 @@
 // Host orchestration only; the kernels live in advect.cu, emit.cu and ftle.cu.
 // Every entry point returns a dpa_status, records a message on failure and
 // never lets a C++ exception cross the boundary.
-#include <cub/device/device_scan.cuh>
-
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
 
+#include "checks.cuh"
 #include "handles.cuh"
 #include "kernels.cuh"
 
@@ -26,16 +27,10 @@ struct dpa_graph {
 
 namespace {
 
-int fail(dpa_context* ctx, int status, const std::string& message) {
-  if (ctx) ctx->error = message;
-  return status;
-}
-
-int fail_cuda(dpa_context* ctx, cudaError_t e, const char* where) {
-  const int status = (e == cudaErrorMemoryAllocation) ? DPA_ERROR_OUT_OF_MEMORY : DPA_ERROR_CUDA;
-  return fail(ctx, status, std::string(where) + ": " + cudaGetErrorName(e) + " (" +
-                               cudaGetErrorString(e) + ")");
-}
+using dpa::check_options;
+using dpa::check_steady;
+using dpa::fail;
+using dpa::fail_cuda;
 
 #define DPA_TRY_CUDA(ctx, expr)                                  \
   do {                                                           \
@@ -81,34 +76,6 @@ cudaStream_t pick_stream(dpa_context* ctx, void* stream) {
   return stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
 }
 
-int check_options(dpa_context* ctx, const dpa_advect_options* o) {
-  if (!o) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "options is NULL");
-  switch (o->integrator) {
-    case DPA_INTEGRATOR_EULER:
-    case DPA_INTEGRATOR_RUNGE_KUTTA_4:
-    case DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE:
-    case DPA_INTEGRATOR_MODIFIED_MIDPOINT:
-    case DPA_INTEGRATOR_RUNGE_KUTTA_CASH_KARP_54:
-    case DPA_INTEGRATOR_RUNGE_KUTTA_DORMAND_PRINCE_5:
-    case DPA_INTEGRATOR_RUNGE_KUTTA_FEHLBERG_78:
-    case DPA_INTEGRATOR_ADAMS_BASHFORTH_2:
-    case DPA_INTEGRATOR_ADAMS_BASHFORTH_MOULTON_2:
-      break;
-    default:
-      return fail(ctx, DPA_ERROR_INVALID_ARGUMENT,
-                  "unknown integrator " + std::to_string(o->integrator));
-  }
-  if (!std::isfinite(o->step_size))
-    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "step_size is not finite");
-  if (o->record && o->max_steps)
-    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "max_steps applies to calls without recording");
-  if (o->max_steps && dpa::integrator_has_history(o->integrator))
-    return fail(ctx, DPA_ERROR_UNSUPPORTED,
-                "max_steps: this integrator carries a derivative from one step to the next, "
-                "so a particle cannot resume in a later call");
-  return DPA_OK;
-}
-
 // Builds the processing order of `count` device positions (coarse Morton
 // buckets, see launch_order) in scratch.values. Returns it through *order.
 int build_order(dpa_context* ctx, dpa_launch_scratch& scratch, const dpa_field* field,
@@ -124,15 +91,6 @@ int build_order(dpa_context* ctx, dpa_launch_scratch& scratch, const dpa_field* 
                                       scratch.values.as<uint32_t>(), stream, ctx->tuning.order));
   ctx->launches += dpa::kOrderLaunches;
   *order = scratch.values.as<uint32_t>();
-  return DPA_OK;
-}
-
-// A time-varying field needs particle times, which only the pathline entry
-// points (and the request server) carry.
-int check_steady(dpa_context* ctx, const dpa_field* field) {
-  if (field->slices > 1)
-    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT,
-                "the field varies in time: advect it with dpa_advect_pathlines_device");
   return DPA_OK;
 }
 
@@ -161,8 +119,7 @@ int advect_device_impl(dpa_context* ctx, const dpa_field* field, const dpa_advec
   dpa::AdvectArgs a{};
   dpa::set_launch_defaults(a);
   if (o->max_steps) a.max_steps = o->max_steps;
-  a.claim = ctx->tuning.claim;
-  a.blocks_per_sm = ctx->tuning.blocks_per_sm;
+  dpa::apply_tuning(ctx->tuning, a);
   a.work_counter = scratch.work_counter.as<unsigned long long>();
   a.count = count;
   a.order = order;
@@ -176,17 +133,8 @@ int advect_device_impl(dpa_context* ctx, const dpa_field* field, const dpa_advec
   if (ctx->profiling) {
     DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->events[2], s));
     ctx->timed_order = true;
+    ctx->timed_round = false;
   }
-  return DPA_OK;
-}
-
-int exclusive_scan(dpa_context* ctx, const uint64_t* in, uint64_t* out, uint64_t count,
-                   cudaStream_t stream) {
-  size_t temp = 0;
-  DPA_TRY_CUDA(ctx, cub::DeviceScan::ExclusiveSum(nullptr, temp, in, out, int64_t(count), stream));
-  DPA_TRY_CUDA(ctx, ctx->scan_temp.reserve(temp));
-  DPA_TRY_CUDA(ctx, cub::DeviceScan::ExclusiveSum(ctx->scan_temp.ptr, temp, in, out,
-                                                  int64_t(count), stream));
   return DPA_OK;
 }
 
@@ -210,7 +158,6 @@ int record_piece(dpa_context* ctx, const dpa_field* field, const dpa_advect_opti
   DPA_TRY_CUDA(ctx, ctx->raw_counts.reserve(n * 8));
   DPA_TRY_CUDA(ctx, ctx->kept_vertices.reserve(n * 4));
   DPA_TRY_CUDA(ctx, ctx->kept_segments.reserve(n * 4));
-  DPA_TRY_CUDA(ctx, ctx->wide.reserve(n * 8));
   DPA_TRY_CUDA(ctx, ctx->vertex_offsets.reserve(n * 8));
   DPA_TRY_CUDA(ctx, ctx->segment_offsets.reserve(n * 8));
   DPA_TRY_CUDA(ctx, ctx->totals.reserve(32));
@@ -221,16 +168,17 @@ int record_piece(dpa_context* ctx, const dpa_field* field, const dpa_advect_opti
   float* positions = ctx->positions.as<float>() + 3 * begin;
   uint64_t* remaining = ctx->remaining.as<uint64_t>() + begin;
   uint8_t* termination = ctx->termination.as<uint8_t>() + begin;
+  if (ctx->profiling) DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->events[0], s));
   const uint32_t* order = nullptr;
   if (o->morton_order && ctx->tuning.order) {
     const int st = build_order(ctx, ctx->scratch, field, positions, n, s, &order);
     if (st != DPA_OK) return st;
   }
+  if (ctx->profiling) DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->events[1], s));
   DPA_TRY_CUDA(ctx, ctx->scratch.work_counter.reserve(sizeof(unsigned long long)));
   dpa::AdvectArgs a{};
   dpa::set_launch_defaults(a);
-  a.claim = ctx->tuning.claim;
-  a.blocks_per_sm = ctx->tuning.blocks_per_sm;
+  dpa::apply_tuning(ctx->tuning, a);
   a.work_counter = ctx->scratch.work_counter.as<unsigned long long>();
   a.count = n;
   a.order = order;
@@ -244,33 +192,27 @@ int record_piece(dpa_context* ctx, const dpa_field* field, const dpa_advect_opti
   a.kept_segments = ctx->kept_segments.as<uint32_t>();
   DPA_TRY_CUDA(ctx, dpa::launch_advect(field->view, a, o->integrator, true, s));
   ctx->launches += 1;
+  if (ctx->profiling) {
+    DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->events[2], s));
+    DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->events[3], s));
+  }
 
   // Per-particle raw counts, then piece-local offsets of kept vertices and
-  // kept segments.
+  // kept segments and their totals.
   DPA_TRY_CUDA(ctx, dpa::launch_raw_counts(ctx->remaining_in.as<uint64_t>() + begin, remaining, n,
                                            ctx->raw_counts.as<uint64_t>(), s));
-  DPA_TRY_CUDA(ctx, dpa::launch_widen_u32(ctx->kept_vertices.as<uint32_t>(), n,
-                                          ctx->wide.as<uint64_t>(), s));
-  int st = exclusive_scan(ctx, ctx->wide.as<uint64_t>(), ctx->vertex_offsets.as<uint64_t>(), n, s);
-  if (st != DPA_OK) return st;
-  DPA_TRY_CUDA(ctx, dpa::launch_widen_u32(ctx->kept_segments.as<uint32_t>(), n,
-                                          ctx->wide.as<uint64_t>(), s));
-  st = exclusive_scan(ctx, ctx->wide.as<uint64_t>(), ctx->segment_offsets.as<uint64_t>(), n, s);
-  if (st != DPA_OK) return st;
-
+  DPA_TRY_CUDA(ctx, ctx->scan_temp.reserve(dpa::curve_offsets_scratch_bytes(n)));
+  DPA_TRY_CUDA(ctx, dpa::launch_curve_offsets(
+                        ctx->kept_vertices.as<uint32_t>(), ctx->kept_segments.as<uint32_t>(), n,
+                        ctx->scan_temp.ptr, ctx->vertex_offsets.as<uint64_t>(),
+                        ctx->segment_offsets.as<uint64_t>(),
+                        ctx->totals.as<unsigned long long>(), s));
+  ctx->launches += 1 + dpa::kCurveOffsetsLaunches;
   uint64_t* ht = ctx->host_totals.as<uint64_t>();
-  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ht, ctx->vertex_offsets.as<uint64_t>() + (n - 1), 8,
-                                    cudaMemcpyDeviceToHost, s));
-  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ht + 1, ctx->segment_offsets.as<uint64_t>() + (n - 1), 8,
-                                    cudaMemcpyDeviceToHost, s));
-  uint32_t* last_counts = ctx->host_totals.as<uint32_t>() + 4;
-  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(&last_counts[0], ctx->kept_vertices.as<uint32_t>() + (n - 1), 4,
-                                    cudaMemcpyDeviceToHost, s));
-  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(&last_counts[1], ctx->kept_segments.as<uint32_t>() + (n - 1), 4,
-                                    cudaMemcpyDeviceToHost, s));
+  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ht, ctx->totals.ptr, 16, cudaMemcpyDeviceToHost, s));
   DPA_TRY_CUDA(ctx, cudaStreamSynchronize(s));
-  const uint64_t piece_vertices = ht[0] + last_counts[0];
-  const uint64_t piece_segments = ht[1] + last_counts[1];
+  const uint64_t piece_vertices = ht[0];
+  const uint64_t piece_segments = ht[1];
   const uint64_t piece_indices = 2 * piece_segments;
   if (!o->index64 && *round_vertices + piece_vertices > 0xffffffffull)
     return fail(ctx, DPA_ERROR_UNSUPPORTED,
@@ -298,6 +240,8 @@ int record_piece(dpa_context* ctx, const dpa_field* field, const dpa_advect_opti
   e.colors = o->colors ? ctx->out_colors.as<float>() : nullptr;
   e.indices = ctx->out_indices.ptr;
   DPA_TRY_CUDA(ctx, dpa::launch_emit(e, o->index64 != 0, o->colors != 0, s));
+  ctx->launches += 1;
+  if (ctx->profiling) DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->events[4], s));
   DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->host_vertices.ptr, ctx->out_vertices.ptr,
                                     piece_vertices * 12, cudaMemcpyDeviceToHost, s));
   if (o->colors)
@@ -306,6 +250,15 @@ int record_piece(dpa_context* ctx, const dpa_field* field, const dpa_advect_opti
   DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->host_indices.ptr, ctx->out_indices.ptr,
                                     piece_indices * index_bytes, cudaMemcpyDeviceToHost, s));
   DPA_TRY_CUDA(ctx, cudaStreamSynchronize(s));
+  if (ctx->profiling) {
+    float order_ms = 0.0f, advect_ms = 0.0f, emit_ms = 0.0f;
+    DPA_TRY_CUDA(ctx, cudaEventElapsedTime(&order_ms, ctx->events[0], ctx->events[1]));
+    DPA_TRY_CUDA(ctx, cudaEventElapsedTime(&advect_ms, ctx->events[1], ctx->events[2]));
+    DPA_TRY_CUDA(ctx, cudaEventElapsedTime(&emit_ms, ctx->events[3], ctx->events[4]));
+    ctx->round_order_ms += order_ms;
+    ctx->round_advect_ms += advect_ms;
+    ctx->round_emit_ms += emit_ms;
+  }
 
   if (sink) {
     dpa_curve_chunk c{};
@@ -402,11 +355,17 @@ int dpa_context_set_profiling(dpa_context* ctx, int32_t enabled) {
     for (cudaEvent_t& e : ctx->events) DPA_TRY_CUDA(ctx, cudaEventCreate(&e));
   ctx->profiling = enabled != 0;
   ctx->timed_order = false;
+  ctx->timed_round = false;
   return DPA_OK;
 }
 
 int dpa_context_last_timing(dpa_context* ctx, float* order_ms, float* advect_ms) {
   if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  if (ctx->profiling && ctx->timed_round) {
+    if (order_ms) *order_ms = ctx->round_order_ms;
+    if (advect_ms) *advect_ms = ctx->round_advect_ms;
+    return DPA_OK;
+  }
   if (!ctx->profiling || !ctx->timed_order)
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "no profiled advection since profiling was enabled");
   DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -417,6 +376,65 @@ int dpa_context_last_timing(dpa_context* ctx, float* order_ms, float* advect_ms)
   if (order_ms) *order_ms = a;
   if (advect_ms) *advect_ms = b;
   return DPA_OK;
+}
+
+int dpa_context_last_emit_timing(dpa_context* ctx, float* emit_ms) {
+  if (!ctx || !emit_ms) return DPA_ERROR_INVALID_ARGUMENT;
+  if (!ctx->profiling || !ctx->timed_round)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT,
+                "no profiled recording round since profiling was enabled");
+  *emit_ms = ctx->round_emit_ms;
+  return DPA_OK;
+}
+
+int dpa_measure_gather_bandwidth(dpa_context* ctx, uint64_t table_bytes, int32_t pattern,
+                                 double* gigabytes_per_second) {
+  if (!ctx || !gigabytes_per_second) return DPA_ERROR_INVALID_ARGUMENT;
+  if (pattern != 0 && pattern != 1)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "pattern must be 0 (coalesced) or 1 (random)");
+  // A cube of 2^(3 side) 16-byte nodes, the largest that fits table_bytes.
+  uint32_t side = 1;
+  while (side < 10 && (16ull << (3 * (side + 1))) <= table_bytes) ++side;
+  const uint64_t nodes = 1ull << (3 * side);
+  if ((16ull << 3) > table_bytes)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "table_bytes below 128");
+  return guarded(ctx, [&]() -> int {
+    DPA_TRY_CUDA(ctx, cudaSetDevice(ctx->device));
+    cudaStream_t s = ctx->stream;
+    DeviceBuffer table, sink;
+    DPA_TRY_CUDA(ctx, table.reserve(nodes * 16));
+    DPA_TRY_CUDA(ctx, sink.reserve(16));
+    DPA_TRY_CUDA(ctx, cudaMemsetAsync(table.ptr, 0, nodes * 16, s));
+    int sms = 0;
+    DPA_TRY_CUDA(ctx, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+    const uint32_t blocks = uint32_t(sms) * 8, iterations = 512;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    DPA_TRY_CUDA(ctx, cudaEventCreate(&e0));
+    const cudaError_t made = cudaEventCreate(&e1);
+    if (made != cudaSuccess) {
+      cudaEventDestroy(e0);
+      return fail_cuda(ctx, made, "cudaEventCreate");
+    }
+    float best = 0.0f;
+    cudaError_t e = cudaSuccess;
+    for (int rep = 0; rep < 4 && e == cudaSuccess; ++rep) {
+      e = cudaEventRecord(e0, s);
+      if (e == cudaSuccess)
+        e = dpa::launch_gather_probe(table.as<float4>(), uint32_t(nodes - 1), side, iterations,
+                                     pattern, sink.as<float>(), blocks, s);
+      if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.0f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e == cudaSuccess && rep > 0 && (best == 0.0f || ms < best)) best = ms;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (e != cudaSuccess) return fail_cuda(ctx, e, "gather probe");
+    const double bytes = double(blocks) * 256.0 * iterations * 8.0 * 16.0;
+    *gigabytes_per_second = bytes / (double(best) * 1e-3) / 1e9;
+    return DPA_OK;
+  });
 }
 
 int dpa_context_launch_count(const dpa_context* ctx, uint64_t* launches) {
@@ -450,6 +468,37 @@ int dpa_integrator_from_name(const char* name, int32_t* integrator) {
   return DPA_ERROR_INVALID_ARGUMENT;
 }
 
+// Whether dividing by h through its rounded reciprocal (Markstein's division,
+// divide_by_reciprocal) gives IEEE division's bits for every float dividend:
+// checked once per divisor and process on the device, over all 2^32 bit
+// patterns (a few milliseconds), and remembered.
+static int reciprocal_divides_exactly(dpa_context* ctx, float h, bool* exact) {
+  static std::mutex lock;
+  static std::map<uint32_t, bool> known;
+  uint32_t bits = 0;
+  std::memcpy(&bits, &h, sizeof bits);
+  {
+    std::lock_guard<std::mutex> guard(lock);
+    const auto it = known.find(bits);
+    if (it != known.end()) {
+      *exact = it->second;
+      return DPA_OK;
+    }
+  }
+  DeviceBuffer counter;
+  DPA_TRY_CUDA(ctx, counter.reserve(sizeof(unsigned int)));
+  DPA_TRY_CUDA(ctx, dpa::launch_verify_division(h, 1.0f / h, counter.as<unsigned int>(),
+                                                ctx->stream));
+  unsigned int mismatches = 0;
+  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(&mismatches, counter.ptr, sizeof mismatches,
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+  DPA_TRY_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  *exact = mismatches == 0;
+  std::lock_guard<std::mutex> guard(lock);
+  known[bits] = *exact;
+  return DPA_OK;
+}
+
 static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
                         const uint64_t shape[3], const float offset[3], const float spacing[3],
                         int32_t storage, dpa_field** out, uint32_t slices = 1,
@@ -470,8 +519,9 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
                      !std::isfinite(time_origin)))
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "time spacing must be positive and finite");
   const uint64_t slice_nodes = shape[0] * shape[1] * shape[2];
-  if (slice_nodes > (1ull << 33) || slice_nodes * slices > (1ull << 33))
-    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "field too large");
+  if (slice_nodes >= (1ull << 32) || slice_nodes * slices > (1ull << 36))
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT,
+                "field too large: at most 2^32 - 1 nodes per slice and 2^36 in all");
   const uint64_t nodes = slice_nodes * slices;
   if (nodes && !xyzv) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "field data is NULL");
   return guarded(ctx, [&]() -> int {
@@ -510,14 +560,26 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
       v.n[i] = int32_t(shape[i]);
       v.offset[i] = offset[i];
       v.spacing[i] = spacing[i];
-      v.inv_spacing[i] = 1.0f / spacing[i];
-      v.scaled_offset[i] = offset[i] * v.inv_spacing[i];
+      v.reciprocal[i] = 1.0f / spacing[i];
+      v.scaled_offset[i] = offset[i] * v.reciprocal[i];
       v.upper[i] = float(int64_t(shape[i]) - 1);
     }
-    v.stride0 = int64_t(shape[1]) * int64_t(shape[2]);
-    v.stride1 = int32_t(shape[2]);
+    v.stride0 = uint32_t(shape[1] * shape[2]);
+    v.stride1 = uint32_t(shape[2]);
     v.storage = storage;
-    v.pow2 = pow2 ? 1 : 0;
+    v.locate = dpa::kLocatePow2;
+    if (!pow2) {
+      bool exact = true;
+      for (int i = 0; i < 3 && exact; ++i) {
+        const int st = reciprocal_divides_exactly(ctx, spacing[i], &exact);
+        if (st != DPA_OK) {
+          f->nodes.release();
+          delete f;
+          return st;
+        }
+      }
+      v.locate = exact ? dpa::kLocateReciprocal : dpa::kLocateDivide;
+    }
     f->slices = slices;
     f->time_origin = time_origin;
     f->time_spacing = time_spacing;
@@ -525,6 +587,18 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
     v.slice_stride = int64_t(slice_nodes);
     v.time_origin = time_origin;
     v.time_spacing = slices > 1 ? time_spacing : 1.0f;
+    v.time_reciprocal = 1.0f / v.time_spacing;
+    v.time_fast = 0;
+    if (slices > 1) {
+      bool exact = false;
+      const int st = reciprocal_divides_exactly(ctx, v.time_spacing, &exact);
+      if (st != DPA_OK) {
+        f->nodes.release();
+        delete f;
+        return st;
+      }
+      v.time_fast = exact ? 1 : 0;
+    }
     v.time_upper = float(int64_t(slices) - 1);
     *out = f;
     return DPA_OK;
@@ -631,6 +705,7 @@ int dpa_advect_round(dpa_context* ctx, const dpa_field* field, const dpa_advect_
       DPA_TRY_CUDA(ctx, ctx->remaining_in.reserve(count * 8));
       DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->remaining_in.ptr, ctx->remaining.ptr, count * 8,
                                         cudaMemcpyDeviceToDevice, s));
+      ctx->round_order_ms = ctx->round_advect_ms = ctx->round_emit_ms = 0.0f;
       // Pieces of the round whose unpruned curves fit the staging limit.
       const uint64_t limit_vertices = std::max<uint64_t>(ctx->staging_limit / 12, 1);
       uint64_t round_vertices = 0, round_indices = 0;
@@ -645,6 +720,10 @@ int dpa_advect_round(dpa_context* ctx, const dpa_field* field, const dpa_advect_
                           &round_indices, end == count, sink, sink_user);
         if (st != DPA_OK) return st;
         begin = end;
+      }
+      if (ctx->profiling) {
+        ctx->timed_round = true;
+        ctx->timed_order = false;
       }
     }
     DPA_TRY_CUDA(ctx, cudaMemcpyAsync(positions, ctx->positions.ptr, count * 12,
@@ -882,9 +961,17 @@ int dpa_context_set_tuning(dpa_context* ctx, const dpa_tuning* tuning) {
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "claim must be in [1, 4096]");
   if (tuning->order > dpa::kOrderMaxResolution)
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "order resolution must be in [0, 64]");
+  if (tuning->block_size % 32 != 0 || tuning->block_size > uint32_t(dpa::kAdvectBlock))
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT,
+                "block_size must be 0 or a multiple of 32 up to " +
+                    std::to_string(dpa::kAdvectBlock));
+  if (tuning->particles_per_thread > 2)
+    return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "particles_per_thread must be 0, 1 or 2");
   ctx->tuning.claim = tuning->claim;
   ctx->tuning.blocks_per_sm = tuning->blocks_per_sm;
   ctx->tuning.order = tuning->order;
+  ctx->tuning.block = tuning->block_size;
+  ctx->tuning.particles_per_thread = tuning->particles_per_thread ? tuning->particles_per_thread : 1;
   return DPA_OK;
 }
 
@@ -894,6 +981,8 @@ int dpa_context_get_tuning(const dpa_context* ctx, dpa_tuning* tuning) {
   tuning->blocks_per_sm = ctx->tuning.blocks_per_sm;
   tuning->order = ctx->tuning.order;
   tuning->measured_ms = 0.0f;
+  tuning->block_size = ctx->tuning.block;
+  tuning->particles_per_thread = ctx->tuning.particles_per_thread;
   return DPA_OK;
 }
 
@@ -940,33 +1029,55 @@ int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_adve
     float winner_ms = 0.0f;
     bool first = true;
     int rc = DPA_OK;
-    const uint32_t claims[] = {16, 32, 64, 128};
-    const uint32_t grids[] = {0, 3, 2};
-    const uint32_t orders[] = {64, 16, 0};
-    for (uint32_t order : orders)
-      for (uint32_t grid : grids)
-        for (uint32_t claim : claims) {
-          ctx->tuning = {claim, grid, order};
-          float best_ms = 0.0f;
-          for (int rep = 0; rep < 3 && rc == DPA_OK; ++rep) {
-            cudaMemcpyAsync(pos.ptr, pos0.ptr, n * 12, cudaMemcpyDeviceToDevice, s);
-            cudaMemcpyAsync(rem.ptr, rem0.ptr, n * 8, cudaMemcpyDeviceToDevice, s);
-            cudaEventRecord(e0, s);
-            rc = advect_device_impl(ctx, field, &o, n, pos.as<float>(), rem.as<uint64_t>(),
-                                    term.as<uint8_t>(), s);
-            cudaEventRecord(e1, s);
-            cudaEventSynchronize(e1);
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (rep > 0 && (best_ms == 0.0f || ms < best_ms)) best_ms = ms;
-          }
-          if (rc != DPA_OK) break;
-          if (first || best_ms < winner_ms) {
-            winner = ctx->tuning;
-            winner_ms = best_ms;
-            first = false;
-          }
-        }
+    // Best of three timed runs (after one untimed) of the sample at the
+    // current ctx->tuning; keeps it as the winner when it is the fastest yet.
+    auto trial = [&]() {
+      float best_ms = 0.0f;
+      for (int rep = 0; rep < 3 && rc == DPA_OK; ++rep) {
+        cudaMemcpyAsync(pos.ptr, pos0.ptr, n * 12, cudaMemcpyDeviceToDevice, s);
+        cudaMemcpyAsync(rem.ptr, rem0.ptr, n * 8, cudaMemcpyDeviceToDevice, s);
+        cudaEventRecord(e0, s);
+        rc = advect_device_impl(ctx, field, &o, n, pos.as<float>(), rem.as<uint64_t>(),
+                                term.as<uint8_t>(), s);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0 && (best_ms == 0.0f || ms < best_ms)) best_ms = ms;
+      }
+      if (rc == DPA_OK && (first || best_ms < winner_ms)) {
+        winner = ctx->tuning;
+        winner_ms = best_ms;
+        first = false;
+      }
+    };
+    // Coordinate search from the defaults: processing order, then the launch
+    // shape (threads per block and particles per lane), then claim size and
+    // blocks per SM, each step keeping the best setting so far.
+    for (uint32_t order : {64u, 16u, 0u}) {
+      if (rc != DPA_OK) break;
+      ctx->tuning = dpa_tuning_state{};
+      ctx->tuning.order = order;
+      trial();
+    }
+    const dpa_tuning_state after_order = winner;
+    for (uint32_t block : {256u, 128u, 64u})
+      for (uint32_t ppt : {1u, 2u}) {
+        if (rc != DPA_OK) break;
+        ctx->tuning = after_order;
+        ctx->tuning.block = block;
+        ctx->tuning.particles_per_thread = ppt;
+        trial();
+      }
+    const dpa_tuning_state after_shape = winner;
+    for (uint32_t grid : {0u, 3u, 2u})
+      for (uint32_t claim : {16u, 32u, 64u, 128u}) {
+        if (rc != DPA_OK) break;
+        ctx->tuning = after_shape;
+        ctx->tuning.blocks_per_sm = grid;
+        ctx->tuning.claim = claim;
+        trial();
+      }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     ctx->profiling = profiling;
@@ -977,6 +1088,8 @@ int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_adve
       best->blocks_per_sm = winner.blocks_per_sm;
       best->order = winner.order;
       best->measured_ms = winner_ms;
+      best->block_size = winner.block;
+      best->particles_per_thread = winner.particles_per_thread;
     }
     return DPA_OK;
   });
@@ -1061,7 +1174,12 @@ int dpa_graph_create_advect(dpa_context* ctx, const dpa_field* field,
     DPA_TRY_CUDA(ctx, g->scratch.values.reserve(count * 4));
     DPA_TRY_CUDA(ctx, g->scratch.sort_temp.reserve(dpa::kOrderCountsSize * 4));
     DPA_TRY_CUDA(ctx, g->scratch.work_counter.reserve(sizeof(unsigned long long)));
-    DPA_TRY_CUDA(ctx, dpa::prepare_advect(field->view, options->integrator, false));
+    {
+      dpa::AdvectArgs launch{};
+      dpa::set_launch_defaults(launch);
+      dpa::apply_tuning(ctx->tuning, launch);
+      DPA_TRY_CUDA(ctx, dpa::prepare_advect(field->view, launch, options->integrator, false));
+    }
     DPA_TRY_CUDA(ctx, cudaStreamSynchronize(s));
     const bool profiling = ctx->profiling;
     ctx->profiling = false;

@@ -24,31 +24,62 @@ constexpr float kTerminal = -2.0f;
 // (particle_advector.cpp:363 tests |v_i| <= 1 * 1e-5 for every component).
 constexpr float kZeroPrecision = 1e-5f;
 
+// How a kernel divides a position by the spacing (per field, every axis):
+//   kLocateDivide      IEEE division (__fdiv_rn);
+//   kLocateReciprocal  a / h as one product by y = RN(1 / h) and one FMA
+//                      correction (Markstein's division), used only for
+//                      divisors for which it was checked at field creation to
+//                      equal __fdiv_rn for every finite float a;
+//   kLocatePow2        power-of-two spacing: one FMA of the exact p / h and
+//                      offset / h, and fmod(p - offset, h) / h = q - floor(q).
+enum LocateMode : int { kLocateDivide = 0, kLocateReciprocal = 1, kLocatePow2 = 2 };
+
 // Device view of a repacked field. Nodes are 4-wide (x, y, z, pad) so one
 // vector load fetches a node: float4 for F32, four 16-bit values for F16/BF16.
+// A slice holds fewer than 2^32 nodes, so a node's index within its slice is
+// a 32-bit value (s0 * stride0 + s1 * stride1 + s2).
 struct FieldView {
   const void* nodes;
   int32_t n[3];        // grid shape
-  int64_t stride0;     // n1 * n2
-  int32_t stride1;     // n2
+  uint32_t stride0;    // n1 * n2
+  uint32_t stride1;    // n2
   float offset[3];
   float spacing[3];
-  float inv_spacing[3];    // exact reciprocals, used only when pow2 is set
-  float scaled_offset[3];  // offset / spacing, exact; used only when pow2 is set
+  float reciprocal[3];     // RN(1 / spacing): exact for power-of-two spacings
+  float scaled_offset[3];  // offset / spacing, exact; used by kLocatePow2 only
   float upper[3];          // n - 1: inside iff 0 <= (p - offset) / h < n - 1
   int32_t storage;         // dpa_storage
-  // Every spacing is a power of two in [2^-20, 2^20] and every offset is zero
-  // or at least 2^-100 in magnitude: (p - offset) / h is then one rounding of
-  // p / h - offset / h, and fmod(p - offset, h) / h is q - floor(q).
-  int32_t pow2;
+  // LocateMode of the spatial axes. kLocatePow2 needs every spacing a power
+  // of two in [2^-20, 2^20] and every offset zero or at least 2^-100 in
+  // magnitude: (p - offset) / h is then one rounding of p / h - offset / h.
+  int32_t locate;
   // Time-varying fields: `slices` grids of slice_stride nodes each, slice s
   // at time time_origin + s * time_spacing; slices == 1 for a steady field.
   int32_t slices;
   int64_t slice_stride;
   float time_origin;
   float time_spacing;
+  float time_reciprocal;   // RN(1 / time_spacing)
+  int32_t time_fast;       // time_reciprocal divides exactly (as kLocateReciprocal)
   float time_upper;      // slices - 1: inside iff 0 <= (t - t0) / dt < slices - 1
 };
+
+// a / h with y = RN(1 / h): q0 = RN(a y), r = a - q0 h (exact, one FMA),
+// q = RN(q0 + r y). Markstein's division ("Computation of elementary functions
+// on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990);
+// its result is used only for divisors verified to equal IEEE division for
+// every finite dividend (verify_reciprocal_division, emit.cu).
+__device__ __forceinline__ float divide_by_reciprocal(float a, float h, float y) {
+  const float q0 = __fmul_rn(a, y);
+  const float r = __fmaf_rn(-q0, h, a);
+  return __fmaf_rn(r, y, q0);
+}
+
+template <int kLocate>
+__device__ __forceinline__ float divide_spacing(float a, float h, float y) {
+  if constexpr (kLocate == kLocateDivide) return __fdiv_rn(a, h);
+  else return divide_by_reciprocal(a, h, y);
+}
 
 // Integrator id of the kernel instantiation shared by the reference's other
 // odeint steppers (modified_midpoint, runge_kutta_cash_karp54,

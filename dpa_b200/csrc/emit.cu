@@ -146,9 +146,117 @@ __global__ void raw_counts_kernel(const uint64_t* in, const uint64_t* out, uint6
   if (t < count) raw[t] = in[t] - out[t] + 2;
 }
 
-__global__ void widen_kernel(const uint32_t* in, uint64_t count, uint64_t* out) {
-  const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t < count) out[t] = in[t];
+// Curve offsets: the exclusive scans of the per-particle kept-vertex and
+// kept-segment counts (uint32) into uint64 offsets, the data-parallel form of
+// the running positions that index_generator::generate (index_generator.cpp:
+// 10-39) and prune_integral_curves walk serially. Three passes over tiles of
+// kScanTileItems particles: tile sums, one block's scan of the tile sums
+// (which also writes the two totals), and each tile's scan plus its prefix.
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;  // consecutive particles per thread
+constexpr uint64_t kScanTileItems = uint64_t(kScanThreads) * kScanItems;
+
+// Block-wide exclusive scan of one pair of values per thread; returns the
+// block's totals through total.
+__device__ __forceinline__ ulonglong2 block_exclusive_scan2(ulonglong2 v, ulonglong2* warp_sums,
+                                                           ulonglong2* total) {
+  const unsigned lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  ulonglong2 x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long a = __shfl_up_sync(0xffffffffu, x.x, o);
+    const unsigned long long b = __shfl_up_sync(0xffffffffu, x.y, o);
+    if (lane >= unsigned(o)) {
+      x.x += a;
+      x.y += b;
+    }
+  }
+  if (lane == 31) warp_sums[warp] = x;
+  __syncthreads();
+  ulonglong2 before = make_ulonglong2(0, 0), all = make_ulonglong2(0, 0);
+  for (unsigned w = 0; w < blockDim.x / 32; ++w) {
+    const ulonglong2 ws = warp_sums[w];
+    if (w < warp) {
+      before.x += ws.x;
+      before.y += ws.y;
+    }
+    all.x += ws.x;
+    all.y += ws.y;
+  }
+  __syncthreads();  // warp_sums may be reused by the caller's next scan
+  *total = all;
+  return make_ulonglong2(before.x + x.x - v.x, before.y + x.y - v.y);
+}
+
+__device__ __forceinline__ ulonglong2 load_counts(const uint32_t* a, const uint32_t* b,
+                                                  uint64_t n, uint64_t i) {
+  return i < n ? make_ulonglong2(a[i], b[i]) : make_ulonglong2(0, 0);
+}
+
+__global__ void __launch_bounds__(kScanThreads) offsets_tile_sums_kernel(
+    const uint32_t* a, const uint32_t* b, uint64_t n, ulonglong2* tile_sums) {
+  __shared__ ulonglong2 warp_sums[kScanThreads / 32];
+  const uint64_t first = uint64_t(blockIdx.x) * kScanTileItems;
+  ulonglong2 sum = make_ulonglong2(0, 0);
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {  // coalesced: item j * threads + t
+    const ulonglong2 v = load_counts(a, b, n, first + uint64_t(j) * kScanThreads + threadIdx.x);
+    sum.x += v.x;
+    sum.y += v.y;
+  }
+  ulonglong2 total;
+  block_exclusive_scan2(sum, warp_sums, &total);
+  if (threadIdx.x == 0) tile_sums[blockIdx.x] = total;
+}
+
+// One block: tile sums -> exclusive tile prefixes in place, in chunks of
+// kScanThreads with a running carry; totals receives the grand totals.
+__global__ void __launch_bounds__(kScanThreads) offsets_tile_prefix_kernel(
+    ulonglong2* tile_sums, uint64_t tiles, unsigned long long* totals) {
+  __shared__ ulonglong2 warp_sums[kScanThreads / 32];
+  ulonglong2 carry = make_ulonglong2(0, 0);
+  for (uint64_t base = 0; base < tiles; base += kScanThreads) {
+    const uint64_t i = base + threadIdx.x;
+    const ulonglong2 v = i < tiles ? tile_sums[i] : make_ulonglong2(0, 0);
+    ulonglong2 total;
+    const ulonglong2 ex = block_exclusive_scan2(v, warp_sums, &total);
+    if (i < tiles) tile_sums[i] = make_ulonglong2(carry.x + ex.x, carry.y + ex.y);
+    carry.x += total.x;
+    carry.y += total.y;
+  }
+  if (threadIdx.x == 0) {
+    totals[0] = carry.x;
+    totals[1] = carry.y;
+  }
+}
+
+__global__ void __launch_bounds__(kScanThreads) offsets_tiles_kernel(
+    const uint32_t* a, const uint32_t* b, uint64_t n, const ulonglong2* tile_prefix,
+    uint64_t* out_a, uint64_t* out_b) {
+  __shared__ ulonglong2 warp_sums[kScanThreads / 32];
+  const uint64_t first = uint64_t(blockIdx.x) * kScanTileItems + uint64_t(threadIdx.x) * kScanItems;
+  ulonglong2 v[kScanItems];
+  ulonglong2 sum = make_ulonglong2(0, 0);
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    v[j] = load_counts(a, b, n, first + j);
+    sum.x += v[j].x;
+    sum.y += v[j].y;
+  }
+  ulonglong2 total;
+  const ulonglong2 ex = block_exclusive_scan2(sum, warp_sums, &total);
+  const ulonglong2 prefix = tile_prefix[blockIdx.x];
+  ulonglong2 run = make_ulonglong2(prefix.x + ex.x, prefix.y + ex.y);
+#pragma unroll
+  for (int j = 0; j < kScanItems; ++j) {
+    const uint64_t i = first + j;
+    if (i < n) {
+      out_a[i] = run.x;
+      out_b[i] = run.y;
+    }
+    run.x += v[j].x;
+    run.y += v[j].y;
+  }
 }
 
 template <int kStorage>
@@ -200,10 +308,25 @@ cudaError_t launch_raw_counts(const uint64_t* remaining_in, const uint64_t* rema
   return cudaGetLastError();
 }
 
-cudaError_t launch_widen_u32(const uint32_t* in, uint64_t count, uint64_t* out,
-                             cudaStream_t stream) {
-  if (count == 0) return cudaSuccess;
-  widen_kernel<<<blocks_for(count, 256), 256, 0, stream>>>(in, count, out);
+uint64_t curve_offsets_scratch_bytes(uint64_t count) {
+  return ((count + kScanTileItems - 1) / kScanTileItems) * sizeof(ulonglong2) + 16;
+}
+
+cudaError_t launch_curve_offsets(const uint32_t* kept_vertices, const uint32_t* kept_segments,
+                                 uint64_t count, void* scratch, uint64_t* vertex_offsets,
+                                 uint64_t* segment_offsets, unsigned long long* totals,
+                                 cudaStream_t stream) {
+  if (count == 0) return cudaMemsetAsync(totals, 0, 16, stream);
+  const uint64_t tiles = (count + kScanTileItems - 1) / kScanTileItems;
+  if (tiles > 0x7fffffffull) return cudaErrorInvalidValue;
+  ulonglong2* sums = static_cast<ulonglong2*>(scratch);
+  offsets_tile_sums_kernel<<<unsigned(tiles), kScanThreads, 0, stream>>>(
+      kept_vertices, kept_segments, count, sums);
+  DPA_CUDA_TRY(cudaGetLastError());
+  offsets_tile_prefix_kernel<<<1, kScanThreads, 0, stream>>>(sums, tiles, totals);
+  DPA_CUDA_TRY(cudaGetLastError());
+  offsets_tiles_kernel<<<unsigned(tiles), kScanThreads, 0, stream>>>(
+      kept_vertices, kept_segments, count, sums, vertex_offsets, segment_offsets);
   return cudaGetLastError();
 }
 

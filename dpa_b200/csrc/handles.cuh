@@ -4,7 +4,7 @@
 
 #include <string>
 
-#include "common.cuh"
+#include "kernels.cuh"
 
 namespace dpa {
 
@@ -77,7 +77,20 @@ struct dpa_tuning_state {
   uint32_t blocks_per_sm = 0; // persistent grid: 0 = as many as fit
   uint32_t order = 64;        // processing order: Morton buckets of an order^3
                               // coarsening of the grid (1..64); 0: input order
+  uint32_t block = 0;         // threads per block (multiple of 32, <= 256); 0: 256, or
+                              // fewer so that a small launch reaches every SM
+  uint32_t particles_per_thread = 1;  // 1 or 2 (steady fields without recording)
 };
+
+namespace dpa {
+// The launch parameters of a tuning.
+inline void apply_tuning(const dpa_tuning_state& t, AdvectArgs& a) {
+  a.claim = t.claim;
+  a.blocks_per_sm = t.blocks_per_sm;
+  a.block = t.block;
+  a.particles_per_thread = t.particles_per_thread;
+}
+}  // namespace dpa
 
 // Scratch of one processing-order + advection launch sequence: bucket ids,
 // the order, the counting sort's counters and the claim counter. A context
@@ -103,8 +116,12 @@ struct dpa_context {
   dpa_launch_scratch scratch;
   uint64_t launches = 0;  // kernels this context launched (advection path)
   bool profiling = false;
-  cudaEvent_t events[3] = {nullptr, nullptr, nullptr};  // order, advect begin, advect end
+  // order begin, advect begin, advect end, emission begin, emission end
+  cudaEvent_t events[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   bool timed_order = false;
+  // A profiled recording round: its pieces' times, summed as they finish.
+  bool timed_round = false;
+  float round_order_ms = 0.0f, round_advect_ms = 0.0f, round_emit_ms = 0.0f;
   dpa_tuning_state tuning;
   DeviceBuffer raw, raw_offsets, raw_counts, kept_vertices, kept_segments;
   DeviceBuffer wide, vertex_offsets, segment_offsets, scan_temp, totals;

@@ -25,6 +25,17 @@ constexpr int kAdvectUnsteadyMinBlocks = DPA_ADVECT_UNSTEADY_MIN_BLOCKS;
 #define DPA_ADVECT_TRUE_RK4_MIN_BLOCKS 3
 #endif
 constexpr int kAdvectTrueRk4MinBlocks = DPA_ADVECT_TRUE_RK4_MIN_BLOCKS;
+// Two particles per lane, stepped in lock-step so that one particle's gather
+// overlaps the other's arithmetic: twice the particle state per thread.
+#ifndef DPA_ADVECT_PPT2_MIN_BLOCKS
+#define DPA_ADVECT_PPT2_MIN_BLOCKS 2
+#endif
+constexpr int kAdvectPpt2MinBlocks = DPA_ADVECT_PPT2_MIN_BLOCKS;
+// Launches whose particles would fill fewer blocks than the device has SMs
+// use smaller blocks (1) or keep kAdvectBlock threads per block (0).
+#ifndef DPA_ADVECT_SPREAD
+#define DPA_ADVECT_SPREAD 1
+#endif
 
 struct AdvectArgs {
   uint64_t count;
@@ -38,6 +49,10 @@ struct AdvectArgs {
   uint64_t max_steps;                // step budget of this launch (~0: none)
   uint32_t claim;                    // order entries a warp claims at once
   uint32_t blocks_per_sm;            // persistent grid per SM (0: occupancy maximum)
+  uint32_t block;                    // threads per block: a multiple of 32 up to
+                                     // kAdvectBlock; 0 = kAdvectBlock, or fewer when
+                                     // the particles would not reach every SM
+  uint32_t particles_per_thread;     // 1 or 2 (2: steady fields without recording)
   unsigned long long* work_counter;  // zeroed by the launcher; claims of the order
   // Recording only.
   float* raw_vertices;          // unpruned curve of particle k at raw_offsets[k]
@@ -60,6 +75,8 @@ inline void set_launch_defaults(AdvectArgs& a) {
   a.max_steps = ~0ull;
   a.claim = 16;
   a.blocks_per_sm = 0;
+  a.block = 0;
+  a.particles_per_thread = 1;
   a.resume_only = false;
   a.request_of = nullptr;
   a.in_flight = nullptr;
@@ -74,16 +91,19 @@ cudaError_t launch_expand_ranges(const uint64_t* starts, const uint64_t* firsts,
                                  cudaStream_t stream);
 
 // Picks the kernel instantiation for the field (steady or time-varying,
-// storage, power-of-two spacing), the integrator and recording.
+// storage, locate mode), the integrator, recording and particles per lane.
 cudaError_t launch_advect(const FieldView& f, const AdvectArgs& a, int integrator, bool record,
                           cudaStream_t stream);
-// The time-varying half of launch_advect (advect_unsteady.cu).
-cudaError_t launch_advect_unsteady(const FieldView& f, const AdvectArgs& a, int integrator,
-                                   bool record, cudaStream_t stream);
+// The instantiations of one storage for steady or time-varying fields
+// (advect_f32.cu, advect_f16.cu, advect_bf16.cu).
+template <int kStorage, bool kUnsteady>
+cudaError_t launch_advect_storage(const FieldView& f, const AdvectArgs& a, int integrator,
+                                  bool record, cudaStream_t stream);
 
 // Resolves, outside any stream capture, what launch_advect looks up on its
-// first use of a kernel instantiation (its occupancy).
-cudaError_t prepare_advect(const FieldView& f, int integrator, bool record);
+// first use of a kernel instantiation (its occupancy at the given launch
+// parameters).
+cudaError_t prepare_advect(const FieldView& f, const AdvectArgs& a, int integrator, bool record);
 
 // Processing order: a counting sort of the particles by the Morton code of
 // their start cell on a resolution^3 coarsening of the grid (a memset and
@@ -127,8 +147,27 @@ cudaError_t launch_emit(const EmitArgs& e, bool index64, bool colors, cudaStream
 cudaError_t launch_raw_counts(const uint64_t* remaining_in, const uint64_t* remaining_out,
                               uint64_t count, uint64_t* raw_counts, cudaStream_t stream);
 
-cudaError_t launch_widen_u32(const uint32_t* in, uint64_t count, uint64_t* out,
-                             cudaStream_t stream);
+// Exclusive scans of the per-particle kept-vertex and kept-segment counts
+// into vertex_offsets and segment_offsets (three kernels); totals (device,
+// two entries) receives the sums of both. scratch holds
+// curve_offsets_scratch_bytes(count) bytes.
+uint64_t curve_offsets_scratch_bytes(uint64_t count);
+cudaError_t launch_curve_offsets(const uint32_t* kept_vertices, const uint32_t* kept_segments,
+                                 uint64_t count, void* scratch, uint64_t* vertex_offsets,
+                                 uint64_t* segment_offsets, unsigned long long* totals,
+                                 cudaStream_t stream);
+constexpr int kCurveOffsetsLaunches = 3;
+
+// The data-path probe of dpa_measure_gather_bandwidth: blocks x 256 lanes,
+// each loading 8 16-byte nodes per iteration from table (mask + 1 nodes).
+cudaError_t launch_gather_probe(const float4* table, uint32_t mask, uint32_t side,
+                                uint32_t iterations, int random, float* sink, uint32_t blocks,
+                                cudaStream_t stream);
+
+// Counts into *mismatches (zeroed first) the 32-bit dividends for which
+// divide_by_reciprocal(a, h, y) differs from IEEE division by h.
+cudaError_t launch_verify_division(float h, float y, unsigned int* mismatches,
+                                   cudaStream_t stream);
 
 // Field repack: XYZV float [n][3] -> 4-wide nodes in the given storage.
 cudaError_t launch_repack(const float* xyzv, uint64_t nodes, int storage, void* out,

@@ -17,6 +17,7 @@
 // current, and handed to the kernels.
 #include <mutex>
 
+#include "checks.cuh"
 #include "handles.cuh"
 #include "kernels.cuh"
 
@@ -57,16 +58,6 @@ cudaError_t scratch_on(int device, unsigned char** out) {
   return cudaSuccess;
 }
 
-int refuse(dpa_context* ctx, int status, const char* message) {
-  ctx->error = message;
-  return status;
-}
-
-int refuse_cuda(dpa_context* ctx, cudaError_t e, const char* where) {
-  ctx->error = std::string(where) + ": " + cudaGetErrorName(e);
-  return DPA_ERROR_CUDA;
-}
-
 }  // namespace
 
 extern "C" int dpa_advect_device_no_alloc(dpa_context* ctx, const dpa_field* field,
@@ -75,51 +66,57 @@ extern "C" int dpa_advect_device_no_alloc(dpa_context* ctx, const dpa_field* fie
                                           uint8_t* device_termination, void* stream) {
   if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
   try {
-    if (!options) return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT, "options is NULL");
-    if (!field || field->owner != ctx) return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT, "bad field");
-    if (field->slices > 1)
-      return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT,
-                    "the field varies in time: advect it with dpa_advect_pathlines_device");
+    // The same checks, in the same order, as dpa_advect_device.
+    int st = dpa::check_options(ctx, options);
+    if (st != DPA_OK) return st;
     if (options->record)
-      return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT,
-                    "dpa_advect_device_no_alloc does not record; use dpa_advect_round");
-    if (!((options->integrator >= DPA_INTEGRATOR_EULER &&
-           options->integrator <= DPA_INTEGRATOR_ADAMS_BASHFORTH_MOULTON_2) ||
-          options->integrator == DPA_INTEGRATOR_RUNGE_KUTTA_4_TRUE))
-      return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT, "unknown integrator");
-    if (options->max_steps && dpa::integrator_has_history(options->integrator))
-      return refuse(ctx, DPA_ERROR_UNSUPPORTED,
-                    "max_steps: this integrator carries a derivative from one step to the "
-                    "next, so a particle cannot resume in a later call");
-    if (count > kMaxParticles)
-      return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT,
-                    "dpa_advect_device_no_alloc: count exceeds DPA_NO_ALLOC_MAX_PARTICLES "
-                    "(1048576); split the particles or use dpa_advect_device");
+      return dpa::fail(ctx, DPA_ERROR_INVALID_ARGUMENT,
+                       "dpa_advect_device_no_alloc does not record; use dpa_advect_round");
+    if (!field || field->owner != ctx) return dpa::fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "bad field");
     if (count && (!device_positions || !device_remaining))
-      return refuse(ctx, DPA_ERROR_INVALID_ARGUMENT, "positions or remaining is NULL");
+      return dpa::fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "positions or remaining is NULL");
+    st = dpa::check_steady(ctx, field);
+    if (st != DPA_OK) return st;
+    if (count > kMaxParticles)
+      return dpa::fail(ctx, DPA_ERROR_INVALID_ARGUMENT,
+                       "dpa_advect_device_no_alloc: count exceeds DPA_NO_ALLOC_MAX_PARTICLES "
+                       "(1048576); split the particles or use dpa_advect_device");
     if (count == 0) return DPA_OK;
 
     cudaError_t e = cudaSetDevice(ctx->device);
-    if (e != cudaSuccess) return refuse_cuda(ctx, e, "cudaSetDevice");
+    if (e != cudaSuccess) return dpa::fail_cuda(ctx, e, "cudaSetDevice");
     unsigned char* scratch = nullptr;
     e = scratch_on(ctx->device, &scratch);
-    if (e != cudaSuccess) return refuse_cuda(ctx, e, "cudaGetSymbolAddress");
+    if (e != cudaSuccess) return dpa::fail_cuda(ctx, e, "cudaGetSymbolAddress");
     cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : ctx->stream;
 
+    // The context's tuning applies as it does to dpa_advect_device: launch
+    // shape, claims and processing order (resolution, or input order when 0).
+    if (ctx->profiling) {
+      e = cudaEventRecord(ctx->events[0], s);
+      if (e != cudaSuccess) return dpa::fail_cuda(ctx, e, "cudaEventRecord");
+    }
     const uint32_t* order = nullptr;
-    if (options->morton_order && count >= 2) {
+    if (options->morton_order && ctx->tuning.order && count >= 2) {
       // launch_order starts by zeroing the counters, so what an earlier call
       // left in the shared array does not matter.
       uint32_t* counts = reinterpret_cast<uint32_t*>(scratch + kCountsOffset);
       uint32_t* order_out = reinterpret_cast<uint32_t*>(scratch + kOrderOffset);
       uint32_t* buckets = reinterpret_cast<uint32_t*>(scratch + kBucketsOffset);
-      e = dpa::launch_order(field->view, device_positions, count, buckets, counts, order_out, s);
-      if (e != cudaSuccess) return refuse_cuda(ctx, e, "ordering kernels");
+      e = dpa::launch_order(field->view, device_positions, count, buckets, counts, order_out, s,
+                            ctx->tuning.order);
+      if (e != cudaSuccess) return dpa::fail_cuda(ctx, e, "ordering kernels");
+      ctx->launches += dpa::kOrderLaunches;
       order = order_out;
+    }
+    if (ctx->profiling) {
+      e = cudaEventRecord(ctx->events[1], s);
+      if (e != cudaSuccess) return dpa::fail_cuda(ctx, e, "cudaEventRecord");
     }
     dpa::AdvectArgs a{};
     dpa::set_launch_defaults(a);
     if (options->max_steps) a.max_steps = options->max_steps;
+    dpa::apply_tuning(ctx->tuning, a);
     // launch_advect zeroes the work counter before the kernel starts.
     a.work_counter = reinterpret_cast<unsigned long long*>(scratch + kCounterOffset);
     a.count = count;
@@ -129,9 +126,15 @@ extern "C" int dpa_advect_device_no_alloc(dpa_context* ctx, const dpa_field* fie
     a.termination = device_termination;
     a.coefficients = dpa::make_step_coefficients(options->integrator, options->step_size);
     e = dpa::launch_advect(field->view, a, options->integrator, false, s);
-    if (e != cudaSuccess) return refuse_cuda(ctx, e, "advection kernel");
+    if (e != cudaSuccess) return dpa::fail_cuda(ctx, e, "advection kernel");
+    ctx->launches += 1;
+    if (ctx->profiling) {
+      e = cudaEventRecord(ctx->events[2], s);
+      if (e != cudaSuccess) return dpa::fail_cuda(ctx, e, "cudaEventRecord");
+      ctx->timed_order = true;
+    }
     return DPA_OK;
   } catch (...) {
-    return DPA_ERROR_INTERNAL;
+    return dpa::fail(ctx, DPA_ERROR_INTERNAL, "unexpected exception");
   }
 }

@@ -11,6 +11,11 @@
 
 #include "common.cuh"
 
+// F32 trilinear products as packed FMUL2 pairs (1) or scalar FMULs (0).
+#ifndef DPA_F32_PACKED_LERP
+#define DPA_F32_PACKED_LERP 0
+#endif
+
 namespace dpa {
 
 // One node of the repacked field, widened to FP32.
@@ -77,58 +82,62 @@ struct Weights {
 // is inside iff 0 <= s <= n - 2 on every axis (regular_grid::contains), which
 // for any float q (NaN included) is 0 <= q < n - 1.
 //
-// Power-of-two spacing (FieldView::pow2): q is one FMA of the exact p / h and
-// offset / h, and fmod(a, h) / h = q - s, whose difference is representable;
-// the sign of a zero weight follows q as fmod's follows a.
+// kLocatePow2: q is one FMA of the exact p / h and offset / h, and
+// fmod(a, h) / h = q - s, whose difference is representable; the sign of a
+// zero weight follows q as fmod's follows a.
 //
 // Other spacings: the rounded quotient is either the true integer quotient N
 // or N + 1 (only when a / h lies within half an ulp below N + 1, so that
 // fmod(a, h) >= h / 2). In both cases a - s * h is exactly representable, so
 // one FMA gives it exactly; adding h back in the N + 1 case is exact too.
-__device__ __forceinline__ float weight_general(float a, float s, float h) {
+// Both divisions are IEEE-exact (kLocateDivide) or by the verified reciprocal
+// (kLocateReciprocal), which gives the same bits.
+template <int kLocate>
+__device__ __forceinline__ float weight_general(float a, float s, float h, float y) {
   float r = fmaf(-s, h, a);
   if (r < 0.0f) r = __fadd_rn(r, h);
   if (r == 0.0f) r = copysignf(0.0f, a);
-  return __fdiv_rn(r, h);
+  return divide_spacing<kLocate>(r, h, y);
 }
 
-template <bool kPow2>
-__device__ __forceinline__ bool locate(const FieldView& f, const Position& p, int cell[3],
+// Locates p; node receives the index of the cell's first corner within its
+// slice (meaningful only when p is inside).
+template <int kLocate>
+__device__ __forceinline__ bool locate(const FieldView& f, const Position& p, uint32_t& node,
                                        Weights& w) {
   float q0, q2, q1;
   float a0 = 0.0f;
   float2 a21 = make_float2(0.0f, 0.0f);
-  if constexpr (kPow2) {
+  if constexpr (kLocate == kLocatePow2) {
     // q = p / h - offset / h in one rounding: p / h and offset / h are exact,
     // so this is the reference's rounded (p - offset) scaled by 1 / h.
-    q0 = __fmaf_rn(p.p0, f.inv_spacing[0], -f.scaled_offset[0]);
+    q0 = __fmaf_rn(p.p0, f.reciprocal[0], -f.scaled_offset[0]);
     const float2 q21 =
-        __ffma2_rn(p.p21, make_float2(f.inv_spacing[2], f.inv_spacing[1]),
+        __ffma2_rn(p.p21, make_float2(f.reciprocal[2], f.reciprocal[1]),
                    make_float2(-f.scaled_offset[2], -f.scaled_offset[1]));
     q2 = q21.x;
     q1 = q21.y;
   } else {
     a0 = __fsub_rn(p.p0, f.offset[0]);
     a21 = sum2(p.p21, neg2(make_float2(f.offset[2], f.offset[1])));
-    q0 = __fdiv_rn(a0, f.spacing[0]);
-    q2 = __fdiv_rn(a21.x, f.spacing[2]);
-    q1 = __fdiv_rn(a21.y, f.spacing[1]);
+    q0 = divide_spacing<kLocate>(a0, f.spacing[0], f.reciprocal[0]);
+    q2 = divide_spacing<kLocate>(a21.x, f.spacing[2], f.reciprocal[2]);
+    q1 = divide_spacing<kLocate>(a21.y, f.spacing[1], f.reciprocal[1]);
   }
   const bool inside = (q0 >= 0.0f) && (q0 < f.upper[0]) && (q1 >= 0.0f) && (q1 < f.upper[1]) &&
                       (q2 >= 0.0f) && (q2 < f.upper[2]);
   const float s0 = floorf(q0), s1 = floorf(q1), s2 = floorf(q2);
-  if constexpr (kPow2) {
+  if constexpr (kLocate == kLocatePow2) {
     w.w0 = copysignf(__fsub_rn(q0, s0), q0);
     const float2 d = sum2(make_float2(q2, q1), neg2(make_float2(s2, s1)));
     w.w21 = make_float2(copysignf(d.x, q2), copysignf(d.y, q1));
   } else {
-    w.w0 = weight_general(a0, s0, f.spacing[0]);
-    w.w21 = make_float2(weight_general(a21.x, s2, f.spacing[2]),
-                        weight_general(a21.y, s1, f.spacing[1]));
+    w.w0 = weight_general<kLocate>(a0, s0, f.spacing[0], f.reciprocal[0]);
+    w.w21 = make_float2(weight_general<kLocate>(a21.x, s2, f.spacing[2], f.reciprocal[2]),
+                        weight_general<kLocate>(a21.y, s1, f.spacing[1], f.reciprocal[1]));
   }
-  cell[0] = int(s0);
-  cell[1] = int(s1);
-  cell[2] = int(s2);
+  // Saturating conversions: outside the grid the value is never used.
+  node = __float2uint_rz(s0) * f.stride0 + __float2uint_rz(s1) * f.stride1 + __float2uint_rz(s2);
   return inside;
 }
 
@@ -166,26 +175,36 @@ template <int kStorage>
 using CornersOf =
     std::conditional_t<kStorage == DPA_STORAGE_F32, CornerNodes, CornerEdges>;
 
+// The node type of a storage: one 16-byte float4 (F32) or 8-byte uint2 (F16,
+// BF16) per node.
 template <int kStorage>
-__device__ __forceinline__ int64_t cell_base(const FieldView& f, const int cell[3],
-                                             int64_t slice_base) {
-  return slice_base + int64_t(cell[0]) * f.stride0 + int64_t(cell[1]) * f.stride1 + cell[2];
-}
+using NodeOf = std::conditional_t<kStorage == DPA_STORAGE_F32, float4, uint2>;
+
+// Pointers to the first node of the cell's four edges along axis 2 (corners
+// 2e and 2e + 1 are consecutive nodes): e = dx * 2 + dy.
+template <int kStorage>
+struct CellEdges {
+  const NodeOf<kStorage>* e[4];
+  __device__ __forceinline__ CellEdges(const FieldView& f, uint32_t node, int64_t slice_base) {
+    const NodeOf<kStorage>* base =
+        reinterpret_cast<const NodeOf<kStorage>*>(f.nodes) + slice_base + node;
+    e[0] = base;
+    e[1] = base + f.stride1;
+    e[2] = base + f.stride0;
+    e[3] = e[2] + f.stride1;
+  }
+};
 
 template <int kStorage>
-__device__ __forceinline__ void gather(const FieldView& f, const int cell[3], CornerNodes& k,
+__device__ __forceinline__ void gather(const FieldView& f, uint32_t node, CornerNodes& k,
                                        int64_t slice_base = 0) {
-  const int64_t base = cell_base<kStorage>(f, cell, slice_base);
-  const int64_t s0 = f.stride0, s1 = f.stride1;
+  const CellEdges<kStorage> c(f, node, slice_base);
   float z[8];
-  load_node<kStorage>(f.nodes, base, k.xy[0].x, k.xy[0].y, z[0]);
-  load_node<kStorage>(f.nodes, base + 1, k.xy[1].x, k.xy[1].y, z[1]);
-  load_node<kStorage>(f.nodes, base + s1, k.xy[2].x, k.xy[2].y, z[2]);
-  load_node<kStorage>(f.nodes, base + s1 + 1, k.xy[3].x, k.xy[3].y, z[3]);
-  load_node<kStorage>(f.nodes, base + s0, k.xy[4].x, k.xy[4].y, z[4]);
-  load_node<kStorage>(f.nodes, base + s0 + 1, k.xy[5].x, k.xy[5].y, z[5]);
-  load_node<kStorage>(f.nodes, base + s0 + s1, k.xy[6].x, k.xy[6].y, z[6]);
-  load_node<kStorage>(f.nodes, base + s0 + s1 + 1, k.xy[7].x, k.xy[7].y, z[7]);
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    load_node<kStorage>(c.e[e], 0, k.xy[2 * e].x, k.xy[2 * e].y, z[2 * e]);
+    load_node<kStorage>(c.e[e], 1, k.xy[2 * e + 1].x, k.xy[2 * e + 1].y, z[2 * e + 1]);
+  }
   k.z04 = make_float2(z[0], z[4]);
   k.z15 = make_float2(z[1], z[5]);
   k.z26 = make_float2(z[2], z[6]);
@@ -193,18 +212,16 @@ __device__ __forceinline__ void gather(const FieldView& f, const int cell[3], Co
 }
 
 template <int kStorage>
-__device__ __forceinline__ void gather(const FieldView& f, const int cell[3], CornerEdges& k,
+__device__ __forceinline__ void gather(const FieldView& f, uint32_t node, CornerEdges& k,
                                        int64_t slice_base = 0) {
-  const int64_t base = cell_base<kStorage>(f, cell, slice_base);
-  const int64_t s0 = f.stride0, s1 = f.stride1;
-  const int64_t edge[4] = {base, base + s1, base + s0, base + s0 + s1};
+  const CellEdges<kStorage> c(f, node, slice_base);
 #pragma unroll
   for (int e = 0; e < 4; ++e) {
     float lo[3], hi[3];
-    load_node<kStorage>(f.nodes, edge[e], lo[0], lo[1], lo[2]);
-    load_node<kStorage>(f.nodes, edge[e] + 1, hi[0], hi[1], hi[2]);
+    load_node<kStorage>(c.e[e], 0, lo[0], lo[1], lo[2]);
+    load_node<kStorage>(c.e[e], 1, hi[0], hi[1], hi[2]);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) k.z[e][c] = make_float2(lo[c], hi[c]);
+    for (int c2 = 0; c2 < 3; ++c2) k.z[e][c2] = make_float2(lo[c2], hi[c2]);
   }
 }
 
@@ -216,7 +233,11 @@ __device__ __forceinline__ void trilinear(const CornerNodes& k, const Weights& w
   const float2 W1 = splat(w.w21.y), T1 = splat(t21.y);
   const float2 W0 = splat(w.w0), T0 = splat(t0);
   auto lerp = [](float2 lo, float2 hi, float2 t, float2 u) {
+#if DPA_F32_PACKED_LERP
+    return add2(mul2(t, lo), mul2(u, hi));
+#else
     return add2(mul2_scalar(t, lo), mul2_scalar(u, hi));
+#endif
   };
   const float2 e0 = lerp(k.xy[0], k.xy[1], T2, W2);
   const float2 e1 = lerp(k.xy[2], k.xy[3], T2, W2);
@@ -258,30 +279,28 @@ __device__ __forceinline__ void trilinear(const CornerEdges& k, const Weights& w
 // A per-thread cache of the current cell's corners: a particle usually stays
 // in one cell for several steps, and the sampled values do not depend on
 // whether the corners came from the cache or from memory.
-template <int kStorage, bool kPow2>
+template <int kStorage, int kLocate>
 struct CellSampler {
   CornersOf<kStorage> corners;
-  int cached[3] = {-1, -1, -1};
+  uint32_t cached = ~0u;  // first node of the cached cell (no cell starts there)
 
   // Samples at p (a steady field: the time t is not used); returns false
   // when p is outside the grid. The sample is returned as v01 = (v0, v1)
   // and v2.
   __device__ __forceinline__ bool sample(const FieldView& f, const Position& p, float /*t*/,
                                          float2& v01, float& v2) {
-    int cell[3];
+    uint32_t node;
     Weights w;
-    if (!locate<kPow2>(f, p, cell, w)) return false;
-    if (cell[0] != cached[0] || cell[1] != cached[1] || cell[2] != cached[2]) {
-      gather<kStorage>(f, cell, corners);
-      cached[0] = cell[0];
-      cached[1] = cell[1];
-      cached[2] = cell[2];
+    if (!locate<kLocate>(f, p, node, w)) return false;
+    if (node != cached) {
+      gather<kStorage>(f, node, corners);
+      cached = node;
     }
     trilinear(corners, w, v01, v2);
     return true;
   }
 
-  __device__ __forceinline__ void reset() { cached[0] = cached[1] = cached[2] = -1; }
+  __device__ __forceinline__ void reset() { cached = ~0u; }
 };
 
 // The time axis of a time-varying field, located by the spatial rule: slice
@@ -290,10 +309,15 @@ struct CellSampler {
 __device__ __forceinline__ bool locate_time(const FieldView& f, float t, int64_t& slice_base,
                                             float& w) {
   const float a = __fsub_rn(t, f.time_origin);
-  const float q = __fdiv_rn(a, f.time_spacing);
+  const float y = f.time_reciprocal;
+  const float q = f.time_fast ? divide_by_reciprocal(a, f.time_spacing, y)
+                              : __fdiv_rn(a, f.time_spacing);
   if (!(q >= 0.0f && q < f.time_upper)) return false;
   const float s = floorf(q);
-  w = weight_general(a, s, f.time_spacing);
+  float r = fmaf(-s, f.time_spacing, a);
+  if (r < 0.0f) r = __fadd_rn(r, f.time_spacing);
+  if (r == 0.0f) r = copysignf(0.0f, a);
+  w = f.time_fast ? divide_by_reciprocal(r, f.time_spacing, y) : __fdiv_rn(r, f.time_spacing);
   slice_base = int64_t(s) * f.slice_stride;
   return true;
 }
@@ -304,27 +328,24 @@ __device__ __forceinline__ bool locate_time(const FieldView& f, float t, int64_t
 // usually stays in one cell for many steps and in one slice pair for many
 // more, and the sampled values do not depend on whether the corners came
 // from the cache or from memory.
-template <int kStorage, bool kPow2>
+template <int kStorage, int kLocate>
 struct TimeSampler {
   CornersOf<kStorage> lo, hi;  // slices s and s + 1
-  int cached[3] = {-1, -1, -1};
+  uint32_t cached = ~0u;
   int64_t cached_slice = -1;
 
   __device__ __forceinline__ bool sample(const FieldView& f, const Position& p, float t,
                                          float2& v01, float& v2) {
-    int cell[3];
+    uint32_t node;
     Weights w;
-    if (!locate<kPow2>(f, p, cell, w)) return false;
+    if (!locate<kLocate>(f, p, node, w)) return false;
     int64_t slice = 0;
     float wt = 0.0f;
     if (!locate_time(f, t, slice, wt)) return false;
-    if (cell[0] != cached[0] || cell[1] != cached[1] || cell[2] != cached[2] ||
-        slice != cached_slice) {
-      gather<kStorage>(f, cell, lo, slice);
-      gather<kStorage>(f, cell, hi, slice + f.slice_stride);
-      cached[0] = cell[0];
-      cached[1] = cell[1];
-      cached[2] = cell[2];
+    if (node != cached || slice != cached_slice) {
+      gather<kStorage>(f, node, lo, slice);
+      gather<kStorage>(f, node, hi, slice + f.slice_stride);
+      cached = node;
       cached_slice = slice;
     }
     float2 a01, b01;
@@ -338,7 +359,7 @@ struct TimeSampler {
   }
 
   __device__ __forceinline__ void reset() {
-    cached[0] = cached[1] = cached[2] = -1;
+    cached = ~0u;
     cached_slice = -1;
   }
 };

@@ -15,8 +15,8 @@
 // particles have all finished leaves the ticks at once; a second thread with
 // its own stream copies its results out, emits its curve and FTLE and returns
 // it, while the worker's ticks go on.
-#include <cub/device/device_scan.cuh>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
@@ -29,6 +29,7 @@
 #include <tuple>
 #include <vector>
 
+#include "admission.hpp"
 #include "handles.cuh"
 #include "kernels.cuh"
 #include "range_allocator.hpp"
@@ -46,6 +47,7 @@ struct pending {
   dpa_request request;
   std::vector<float> positions;
   double queued;
+  double deadline;  // seconds since the server started; 0: none
 };
 
 struct active_request {
@@ -56,6 +58,7 @@ struct active_request {
   uint64_t raw_count;
   double admitted;
   uint64_t first_tick;   // the first tick that advances it
+  int32_t dropped = DPA_OK;  // DPA_ERROR_TIMEOUT / CANCELLED once dropped while running
 };
 
 struct response_storage {
@@ -92,7 +95,7 @@ struct dpa_server {
   cudaEvent_t seeds_copied = nullptr, readback[2] = {nullptr, nullptr};
   cudaEvent_t tick_start[2] = {nullptr, nullptr};  // device time of each tick
   // Emission scratch.
-  DeviceBuffer raw_counts, wide, vertex_offsets, segment_offsets, scan_temp, out_vertices,
+  DeviceBuffer raw_counts, curve_totals, vertex_offsets, segment_offsets, scan_temp, out_vertices,
       out_colors, out_indices;
   DeviceBuffer ftle_original, ftle_winners, ftle_flow, ftle_out;
   range_allocator slots, vertices;
@@ -102,6 +105,9 @@ struct dpa_server {
   std::condition_variable wake, done_signal;
   std::deque<pending> queue;
   std::vector<active_request> active;
+  uint64_t used_slots = 0;
+  dpa::admission_config admission;
+  std::map<uint64_t, int32_t> drop_requests;  // id -> status, from dpa_server_cancel
   std::map<uint64_t, std::unique_ptr<response_storage>> done, handed_out;
   std::deque<uint64_t> done_order;
   std::thread worker, finisher;
@@ -131,6 +137,8 @@ struct dpa_server {
   }
   uint32_t tick(uint64_t steps, int parity);
   void select(std::vector<active_request>& out);
+  void drop_waiting(double t);
+  void drop_running(double t);
   void upload(std::vector<active_request>& admitted, uint64_t first_tick);
   void finish(active_request& a, response_storage& out);
 };
@@ -167,6 +175,17 @@ __global__ void serve_init_kernel(uint64_t first, uint64_t n, uint64_t iteration
   if (!ordered) seed_order[k] = uint32_t(i);
 }
 
+// Drops a running request between ticks: its particles still in flight are
+// marked cancelled (later ticks skip them) and its in-flight counter is
+// zeroed, so the next read of the counters hands it to the finisher.
+__global__ void serve_drop_kernel(uint64_t first, uint64_t n, uint32_t slot, uint8_t* termination,
+                                  unsigned int* in_flight) {
+  const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (i == 0) in_flight[slot] = 0;
+  if (i < n && termination[first + i] == DPA_TERMINATION_IN_FLIGHT)
+    termination[first + i] = DPA_TERMINATION_CANCELLED;
+}
+
 // Requests of fewer seeds run in submission order: sorting them would cost
 // more launches than their few warps gain in locality.
 constexpr uint64_t kServeOrderMin = 4096;
@@ -182,30 +201,93 @@ bool integrator_ok(int32_t i) {
 
 }  // namespace
 
-// Called with the mutex held: moves the queue's head requests that fit the
-// arenas into `out`, first in, first out (the head waits until they have
-// room for it).
+// Called with the mutex held: moves the waiting requests that may start now
+// into `out` (the policy of admission.hpp: oldest first, younger requests
+// that fit may pass one that does not, within the reserve and bypass limits).
 void dpa_server::select(std::vector<active_request>& out) {
-  while (!queue.empty() && !free_counters.empty()) {
-    pending& head = queue.front();
-    const dpa_request& q = head.request;
-    const uint64_t raw_need = q.record ? q.count * (q.iterations + 2) : 0;
-    uint64_t first = 0, raw_first = 0;
-    if (!slots.allocate(q.count, &first)) break;
-    if (!vertices.allocate(raw_need, &raw_first)) {
-      slots.release(first, q.count);
-      break;
+  const double t = now();
+  uint64_t first = 0, raw_first = 0;
+  dpa::admit_waiting(
+      queue, admission, used_slots, [](const pending& p) { return p.request.count; },
+      [&](const pending& p) { return t - p.queued; },
+      [&](const pending& p) {
+        const dpa_request& q = p.request;
+        const uint64_t raw_need = q.record ? q.count * (q.iterations + 2) : 0;
+        if (!slots.allocate(q.count, &first)) return false;
+        if (!vertices.allocate(raw_need, &raw_first)) {
+          slots.release(first, q.count);
+          return false;
+        }
+        return true;
+      },
+      [&](pending& p) {
+        active_request a;
+        a.raw_count = p.request.record ? p.request.count * (p.request.iterations + 2) : 0;
+        a.p = std::move(p);
+        a.slot = free_counters.back();
+        free_counters.pop_back();
+        a.first = first;
+        a.raw_first = raw_first;
+        a.admitted = t;
+        out.push_back(std::move(a));
+      },
+      [&] { return !free_counters.empty(); });
+}
+
+// Called with the mutex held: returns the waiting requests that have passed
+// their deadline or were cancelled, without arrays.
+void dpa_server::drop_waiting(double t) {
+  for (auto it = queue.begin(); it != queue.end();) {
+    int32_t status = DPA_OK;
+    const auto c = drop_requests.find(it->id);
+    if (c != drop_requests.end()) {
+      status = c->second;
+      drop_requests.erase(c);
+    } else if (it->deadline > 0.0 && t >= it->deadline) {
+      status = DPA_ERROR_TIMEOUT;
     }
-    active_request a;
-    a.p = std::move(head);
-    queue.pop_front();
-    a.slot = free_counters.back();
-    free_counters.pop_back();
-    a.first = first;
-    a.raw_first = raw_first;
-    a.raw_count = raw_need;
-    a.admitted = now();
-    out.push_back(std::move(a));
+    if (status == DPA_OK) {
+      ++it;
+      continue;
+    }
+    auto out = std::make_unique<response_storage>();
+    dpa_response& r = out->r;
+    r.id = it->id;
+    r.user = it->request.user;
+    r.status = status;
+    r.count = it->request.count;
+    r.queued_seconds = it->queued;
+    r.admitted_seconds = t;
+    r.finished_seconds = t;
+    done_order.push_back(r.id);
+    done[r.id] = std::move(out);
+    stats.completed += 1;
+    it = queue.erase(it);
+    done_signal.notify_all();
+  }
+}
+
+// Called with the mutex held, in the worker between ticks: a running request
+// past its deadline or cancelled is dropped on the ticks' stream before the
+// next tick (serve_drop_kernel) and finishes through the usual read of the
+// in-flight counters.
+void dpa_server::drop_running(double t) {
+  for (active_request& a : active) {
+    if (a.dropped != DPA_OK) continue;
+    int32_t status = DPA_OK;
+    const auto c = drop_requests.find(a.p.id);
+    if (c != drop_requests.end()) {
+      status = c->second;
+      drop_requests.erase(c);
+    } else if (a.p.deadline > 0.0 && t >= a.p.deadline) {
+      status = DPA_ERROR_TIMEOUT;
+    }
+    if (status == DPA_OK) continue;
+    a.dropped = status;
+    const uint64_t n = a.p.request.count;
+    serve_drop_kernel<<<unsigned(std::max<uint64_t>((n + 255) / 256, 1)), 256, 0, stream>>>(
+        a.first, n, a.slot, termination.as<uint8_t>(), in_flight.as<unsigned int>());
+    SERVER_TRY(cudaGetLastError());
   }
 }
 
@@ -304,7 +386,7 @@ uint32_t dpa_server::tick(uint64_t steps, int parity) {
     a.termination = termination.as<uint8_t>();
     a.coefficients = dpa::make_step_coefficients(integrator, step_size);
     a.max_steps = steps;
-    a.claim = tuning.claim;
+    dpa::apply_tuning(tuning, a);
     a.work_counter = work_counter.as<unsigned long long>();
     a.resume_only = true;
     a.request_of = request_of.as<uint32_t>();
@@ -343,40 +425,36 @@ void dpa_server::finish(active_request& a, response_storage& out) {
     SERVER_TRY(cudaMemcpyAsync(out.termination.data(), termination.as<uint8_t>() + first, n,
                                cudaMemcpyDeviceToHost, finish_stream));
   }
+  // A request the worker dropped is returned as it stood, without curve or
+  // FTLE -- unless every particle had finished before the drop took effect.
+  int32_t status = DPA_OK;
+  if (a.dropped != DPA_OK) {
+    SERVER_TRY(cudaStreamSynchronize(finish_stream));
+    for (uint64_t i = 0; i < n && status == DPA_OK; ++i)
+      if (out.termination[i] == DPA_TERMINATION_CANCELLED) status = a.dropped;
+  }
   uint64_t vertex_count = 0, index_count = 0;
-  if (q.record && n) {
+  if (q.record && n && status == DPA_OK) {
     // Emission of the request's curve, as one round of the reference.
     SERVER_TRY(raw_counts.reserve(n * 8));
-    SERVER_TRY(wide.reserve(n * 8));
     SERVER_TRY(vertex_offsets.reserve(n * 8));
     SERVER_TRY(segment_offsets.reserve(n * 8));
     SERVER_TRY(dpa::launch_raw_counts(remaining_initial.as<uint64_t>() + first,
                                       remaining.as<uint64_t>() + first, n,
                                       raw_counts.as<uint64_t>(), finish_stream));
-    auto scan = [&](const uint32_t* in, uint64_t* out_offsets) {
-      SERVER_TRY(dpa::launch_widen_u32(in, n, wide.as<uint64_t>(), finish_stream));
-      size_t temp = 0;
-      SERVER_TRY(cub::DeviceScan::ExclusiveSum(nullptr, temp, wide.as<uint64_t>(), out_offsets,
-                                               int64_t(n), finish_stream));
-      SERVER_TRY(scan_temp.reserve(temp));
-      SERVER_TRY(cub::DeviceScan::ExclusiveSum(scan_temp.ptr, temp, wide.as<uint64_t>(),
-                                               out_offsets, int64_t(n), finish_stream));
-    };
-    scan(kept_vertices.as<uint32_t>() + first, vertex_offsets.as<uint64_t>());
-    scan(kept_segments.as<uint32_t>() + first, segment_offsets.as<uint64_t>());
-    uint64_t tail[2];
-    uint32_t last[2];
-    SERVER_TRY(cudaMemcpyAsync(&tail[0], vertex_offsets.as<uint64_t>() + (n - 1), 8,
-                               cudaMemcpyDeviceToHost, finish_stream));
-    SERVER_TRY(cudaMemcpyAsync(&tail[1], segment_offsets.as<uint64_t>() + (n - 1), 8,
-                               cudaMemcpyDeviceToHost, finish_stream));
-    SERVER_TRY(cudaMemcpyAsync(&last[0], kept_vertices.as<uint32_t>() + first + (n - 1), 4,
-                               cudaMemcpyDeviceToHost, finish_stream));
-    SERVER_TRY(cudaMemcpyAsync(&last[1], kept_segments.as<uint32_t>() + first + (n - 1), 4,
-                               cudaMemcpyDeviceToHost, finish_stream));
+    SERVER_TRY(scan_temp.reserve(dpa::curve_offsets_scratch_bytes(n)));
+    SERVER_TRY(curve_totals.reserve(16));
+    SERVER_TRY(dpa::launch_curve_offsets(kept_vertices.as<uint32_t>() + first,
+                                         kept_segments.as<uint32_t>() + first, n, scan_temp.ptr,
+                                         vertex_offsets.as<uint64_t>(),
+                                         segment_offsets.as<uint64_t>(),
+                                         curve_totals.as<unsigned long long>(), finish_stream));
+    uint64_t totals[2];
+    SERVER_TRY(cudaMemcpyAsync(totals, curve_totals.ptr, 16, cudaMemcpyDeviceToHost,
+                               finish_stream));
     SERVER_TRY(cudaStreamSynchronize(finish_stream));
-    vertex_count = tail[0] + last[0];
-    index_count = 2 * (tail[1] + last[1]);
+    vertex_count = totals[0];
+    index_count = 2 * totals[1];
     const size_t index_bytes = q.index64 ? 8 : 4;
     SERVER_TRY(out_vertices.reserve(vertex_count * 12));
     SERVER_TRY(out_colors.reserve(vertex_count * 4));
@@ -414,8 +492,8 @@ void dpa_server::finish(active_request& a, response_storage& out) {
   uint64_t steps = 0;
   for (uint64_t i = 0; i < n; ++i) steps += q.iterations - out.remaining[i];
   dpa_response& r = out.r;
-  r.status = DPA_OK;
-  if (q.ftle && n) {
+  r.status = status;
+  if (q.ftle && n && status == DPA_OK) {
     // Lattice FTLE of the final positions (ftle_estimator.cpp:7-65); the
     // seeds should be the lattice of seed_stride on the request's field.
     const dpa_field* field = fields[size_t(q.field)];
@@ -491,6 +569,9 @@ void dpa_server::run() {
       {
         std::unique_lock<std::mutex> lock(mutex);
         if (!failure.empty()) break;  // the finisher failed
+        const double t = now();
+        drop_waiting(t);
+        drop_running(t);
         select(admitted);
         waiting = !queue.empty();
         if (active.empty() && admitted.empty() && !pending) {
@@ -580,11 +661,13 @@ void dpa_server::run_finisher() {
       finish(a, *out);
       std::lock_guard<std::mutex> lock(mutex);
       slots.release(a.first, a.p.request.count);
+      used_slots -= a.p.request.count;
       vertices.release(a.raw_first, a.raw_count);
       free_counters.push_back(a.slot);
       stats.particle_steps += out->r.particle_steps;
       stats.completed += 1;
       const uint64_t id = out->r.id;
+      drop_requests.erase(id);  // a cancel that arrived after the request finished
       done_order.push_back(id);
       done[id] = std::move(out);
       done_signal.notify_all();
@@ -651,6 +734,11 @@ int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_s
     s->fields.reserve(kMaxServerFields);
     s->slots.reset(p);
     s->vertices.reset(v);
+    s->admission.slot_capacity = p;
+    s->admission.small_seeds = options->small_request_seeds ? options->small_request_seeds : 65536;
+    s->admission.reserved_slots = p / 100 * std::min<uint32_t>(options->reserved_percent, 90);
+    s->admission.max_bypass_seconds =
+        1e-3 * double(options->max_bypass_ms ? options->max_bypass_ms : 250);
     for (uint32_t i = options->max_requests; i-- > 0;) s->free_counters.push_back(i);
     dpa_server* raw_ptr = s.get();
     s->worker = std::thread([raw_ptr] { raw_ptr->run(); });
@@ -700,6 +788,7 @@ int dpa_server_submit(dpa_server* s, const dpa_request* request, uint64_t* id) {
     if (!s->failure.empty() || s->stopping) return DPA_ERROR_INTERNAL;
     p.id = s->next_id++;
     p.queued = s->now();
+    p.deadline = q.deadline_ms ? p.queued + 1e-3 * double(q.deadline_ms) : 0.0;
     *id = p.id;
     s->queue.push_back(std::move(p));
     s->stats.submitted += 1;
@@ -730,6 +819,20 @@ int dpa_server_poll(dpa_server* s, int32_t wait_ms, dpa_response* out, int32_t* 
   s->handed_out[id] = std::move(it->second);
   s->done.erase(it);
   *got = 1;
+  return DPA_OK;
+}
+
+int dpa_server_cancel(dpa_server* s, uint64_t id) {
+  if (!s) return DPA_ERROR_INVALID_ARGUMENT;
+  {
+    std::lock_guard<std::mutex> lock(s->mutex);
+    bool known = false;
+    for (const pending& p : s->queue) known = known || p.id == id;
+    for (const active_request& a : s->active) known = known || a.p.id == id;
+    if (!known) return DPA_ERROR_INVALID_ARGUMENT;  // unknown, finishing or finished
+    s->drop_requests[id] = DPA_ERROR_CANCELLED;
+  }
+  s->wake.notify_one();
   return DPA_OK;
 }
 

@@ -37,11 +37,13 @@ class Server:
     """Continuous-batching request server over resident fields."""
 
     def __init__(self, context, particle_capacity: int, vertex_capacity: int = 0,
-                 steps_per_tick: int = 64, max_requests: int = 256):
+                 steps_per_tick: int = 64, max_requests: int = 256, small_request_seeds: int = 0,
+                 reserved_percent: int = 0, max_bypass_ms: int = 0):
         self.context = context
         self._lib = context._lib
         opts = N.ServerOptions(int(particle_capacity), int(vertex_capacity), int(steps_per_tick),
-                               int(max_requests))
+                               int(max_requests), int(small_request_seeds), int(reserved_percent),
+                               int(max_bypass_ms))
         handle = C.c_void_p()
         context.check(self._lib.dpa_server_create(context.handle, C.byref(opts), C.byref(handle)))
         self.handle = handle
@@ -55,19 +57,25 @@ class Server:
 
     def submit(self, field_id: int, positions, iterations: int, integrator: str = "runge_kutta_4",
                step_size: float = 0.25, record: bool = False, index64: bool = False,
-               ftle: bool = False, seed_stride=(1.0, 1.0, 1.0), start_time: float = 0.0) -> int:
+               ftle: bool = False, seed_stride=(1.0, 1.0, 1.0), start_time: float = 0.0,
+               deadline_ms: int = 0) -> int:
         pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
         req = N.Request(int(field_id), N.INTEGRATORS[integrator], float(np.float32(step_size)),
                         int(record), int(index64), int(ftle),
                         (C.c_float * 3)(*[float(v) for v in seed_stride]), pos.shape[0],
                         pos.ctypes.data_as(C.POINTER(C.c_float)), int(iterations), None,
-                        float(np.float32(start_time)))
+                        float(np.float32(start_time)), int(deadline_ms))
         rid = C.c_uint64()
         status = self._lib.dpa_server_submit(self.handle, C.byref(req), C.byref(rid))
         if status != N.DPA_OK:
             raise N.DpaError(status, "request rejected")
         self._index64[rid.value] = bool(index64)
         return rid.value
+
+    def cancel(self, request_id: int) -> bool:
+        """Asks the server to drop a request; False when it is unknown or
+        already returned."""
+        return self._lib.dpa_server_cancel(self.handle, int(request_id)) == N.DPA_OK
 
     def poll(self, wait_ms: int = 0) -> Result | None:
         r = N.Response()
@@ -76,7 +84,8 @@ class Server:
                 self.context.handle)
         if not got.value:
             return None
-        n = int(r.count)
+        # A request dropped before admission returns no arrays.
+        n = int(r.count) if r.positions else 0
         arr = lambda p, shape: np.ctypeslib.as_array(p, shape=shape).copy() if n else np.zeros(shape)
         pos = arr(r.positions, (n * 3,)).reshape(n, 3).astype(np.float32) if n else np.zeros((0, 3), np.float32)
         rem = arr(r.remaining, (n,)).astype(np.uint64) if n else np.zeros(0, np.uint64)

@@ -37,7 +37,9 @@ typedef enum dpa_status {
   DPA_ERROR_OUT_OF_MEMORY = 3,
   DPA_ERROR_CUDA = 4,
   DPA_ERROR_SINK = 5,
-  DPA_ERROR_INTERNAL = 6
+  DPA_ERROR_INTERNAL = 6,
+  DPA_ERROR_TIMEOUT = 7,   /* a served request passed its deadline and was dropped */
+  DPA_ERROR_CANCELLED = 8  /* a served request was cancelled (dpa_server_cancel) */
 } dpa_status;
 
 /* Device storage of a field. F32 keeps the reference's values exactly; F16 and
@@ -77,7 +79,9 @@ typedef enum dpa_termination {
   DPA_TERMINATION_COMPLETE = 0,      /* remaining_iterations reached 0 */
   DPA_TERMINATION_OUT_OF_BOUNDS = 1, /* regular_grid::contains failed */
   DPA_TERMINATION_ZERO_VELOCITY = 2, /* interpolated vector isZero() */
-  DPA_TERMINATION_IN_FLIGHT = 3      /* stopped by dpa_advect_options.max_steps; resumable */
+  DPA_TERMINATION_IN_FLIGHT = 3,     /* stopped by dpa_advect_options.max_steps; resumable */
+  DPA_TERMINATION_CANCELLED = 4      /* served request dropped (deadline or cancel) while the
+                                        particle was still in flight */
 } dpa_termination;
 
 /* FTLE scatter rule. REFERENCE puts each final position into the flow-map
@@ -150,11 +154,26 @@ int dpa_context_set_staging_limit(dpa_context* ctx, uint64_t bytes);
 
 /* Instrumentation, the counterpart of the reference's per-round timers
  * (pipeline.cpp:98-145, benchmark.hpp:152-158). With profiling on, every
- * non-recording advection records CUDA events on its stream around the
- * ordering kernels and the advection kernel; dpa_context_last_timing waits
- * for the last call's events and returns both durations in milliseconds. */
+ * advection records CUDA events on its stream around the ordering kernels
+ * and the advection kernel (and, in a recording round, around each piece's
+ * emission: curve offsets and emit kernel); dpa_context_last_timing waits for
+ * the last call's events and returns both durations in milliseconds (summed
+ * over the pieces of a recording round), dpa_context_last_emit_timing the
+ * emission time of the last recording round. */
 int dpa_context_set_profiling(dpa_context* ctx, int32_t enabled);
 int dpa_context_last_timing(dpa_context* ctx, float* order_ms, float* advect_ms);
+int dpa_context_last_emit_timing(dpa_context* ctx, float* emit_ms);
+
+/* The device's load bandwidth for the advection kernels' gather pattern:
+ * lanes load the eight 16-byte nodes of one cell (four edges of two
+ * consecutive nodes) per iteration from a table of at most table_bytes.
+ * pattern 0: the lanes of a warp read consecutive cells (the data path's
+ * ceiling); 1: every lane reads a random cell. A table that fits each SM's
+ * L1 (tens of KiB) measures the L1 data path, one that fits L2 (tens of MiB)
+ * the L2 path. Returns node bytes delivered per second, in GB/s. No
+ * counterpart in the reference; it gives the gather roofline its peak. */
+int dpa_measure_gather_bandwidth(dpa_context* ctx, uint64_t table_bytes, int32_t pattern,
+                                 double* gigabytes_per_second);
 
 /* Number of kernels this context has launched on the advection path. */
 int dpa_context_launch_count(const dpa_context* ctx, uint64_t* launches);
@@ -270,18 +289,26 @@ typedef struct dpa_tuning {
   uint32_t order;          /* processing order: Morton buckets of a order^3 coarsening
                               of the grid (1..64), 0 = input order */
   float    measured_ms;    /* dpa_autotune_advect: time of the chosen setting */
+  uint32_t block_size;     /* threads per block, a multiple of 32 up to 256; 0 = 256,
+                              or fewer when a launch's particles would not reach
+                              every SM */
+  uint32_t particles_per_thread; /* 1 or 2 particles stepped together by each lane
+                              (2 applies to steady fields without recording) */
 } dpa_tuning;
 
 int dpa_context_set_tuning(dpa_context* ctx, const dpa_tuning* tuning);
 int dpa_context_get_tuning(const dpa_context* ctx, dpa_tuning* tuning);
 
-/* Times the candidate settings (claim 16..128, 2 to all resident blocks per SM,
- * order 64 / 16 / off) on copies of the first min(count, 4,194,304) of the
- * given device particles, each advanced at most sample_steps steps (0: its
+/* Times candidate settings on copies of the first min(count, 4,194,304) of
+ * the given device particles, each advanced at most sample_steps steps (0: its
  * whole remaining budget, capped by options->max_steps), keeps the fastest in
- * the context and returns it in best (may be NULL). The processing order pays
- * off with particle density and run length, so a sample as dense and as long
- * as the real run picks the setting that run wants. */
+ * the context and returns it in best (may be NULL). The search goes one knob
+ * group at a time from the defaults, keeping the best so far: processing order
+ * (64 / 16 / off), then launch shape (256, 128 or 64 threads per block, one or
+ * two particles per lane), then claim size (16..128) with blocks per SM (all
+ * that fit, 3, 2). The processing order pays off with particle density and run
+ * length, so a sample as dense and as long as the real run picks the setting
+ * that run wants. */
 int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_advect_options* options,
                         uint64_t count, const float* device_positions,
                         const uint64_t* device_remaining, uint64_t sample_steps,
@@ -289,20 +316,34 @@ int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_adve
 
 /* ---- serving (no counterpart in the reference) ------------------------------ */
 
-/* A request server: fields stay resident, requests are admitted first in,
- * first out when the device arenas have room for them (count particle slots;
- * for recording requests also count * (iterations + 2) curve-staging
- * vertices, their output buffer), and admitted requests advance together in
- * ticks of steps_per_tick steps: one persistent launch per group of requests
- * sharing a field, integrator, step size and recording switch. Requests that
- * arrive while others run join at the next tick. A worker thread owns the
- * ticks; a second thread, on its own stream, copies out, emits and returns
- * the requests that have finished while the ticks go on. A request of 4096
- * seeds or more is swept in the Morton order of its seeds' start cells. The
- * launches use the context's tuning (dpa_context_set_tuning) as it was when
- * the server was created; an order of 0 there sweeps requests in submission
- * order. submit, poll and stats may be called from any thread. The context is
- * used for its device, its fields and that tuning only. */
+/* A request server: fields stay resident, and requests are admitted when the
+ * device arenas have room for them (count particle slots; for recording
+ * requests also count * (iterations + 2) curve-staging vertices, their output
+ * buffer). Admission scans the waiting requests oldest first and admits every
+ * one that fits, so a small request does not wait behind a large one that has
+ * no room yet; reserved_percent of the slots are kept for small requests (at
+ * most small_request_seeds seeds), and once the oldest waiting request has
+ * waited max_bypass_ms nothing behind it is admitted before it. Admitted
+ * requests advance together in ticks of steps_per_tick steps: one persistent
+ * launch per group of requests sharing a field, integrator, step size and
+ * recording switch. Requests that arrive while others run join at the next
+ * tick. A worker thread owns the ticks; a second thread, on its own stream,
+ * copies out, emits and returns the requests that have finished while the
+ * ticks go on. A request of 4096 seeds or more is swept in the Morton order
+ * of its seeds' start cells. The launches use the context's tuning
+ * (dpa_context_set_tuning) as it was when the server was created; an order of
+ * 0 there sweeps requests in submission order. submit, poll, cancel and stats
+ * may be called from any thread. The context is used for its device, its
+ * fields and that tuning only.
+ *
+ * Failure handling is on the host: a request with a deadline that has not
+ * finished deadline_ms after its submission, or one cancelled with
+ * dpa_server_cancel, is dropped between ticks (the ticks never wait on the
+ * host inside a kernel) and returned with status DPA_ERROR_TIMEOUT or
+ * DPA_ERROR_CANCELLED: a request dropped while waiting carries no arrays; one
+ * dropped while running carries its particles as they stood (those still in
+ * flight marked DPA_TERMINATION_CANCELLED) and no curve or FTLE. The other
+ * requests are not affected. */
 typedef struct dpa_server_options {
   uint64_t particle_capacity;  /* particle slots of the arena (62 bytes each) */
   uint64_t vertex_capacity;    /* curve-staging vertices of the arena (12 bytes each) */
@@ -310,6 +351,11 @@ typedef struct dpa_server_options {
                                   admission (0: 64); four times as many while
                                   none waits */
   uint32_t max_requests;       /* requests admitted at once */
+  uint64_t small_request_seeds; /* requests of at most this many seeds may use the
+                                  reserved slots (0: 65536) */
+  uint32_t reserved_percent;   /* share of the slots kept for small requests (0-90) */
+  uint32_t max_bypass_ms;      /* how long the oldest waiting request may be passed
+                                  by younger ones that fit (0: 250 ms) */
 } dpa_server_options;
 
 typedef struct dpa_request {
@@ -326,6 +372,8 @@ typedef struct dpa_request {
   void*       user;
   float       start_time;      /* the seeds' time: pathlines through a time-varying
                                   field start there (steady fields: tracked only) */
+  uint32_t    deadline_ms;     /* drop the request if it has not finished this long
+                                  after submission (0: no deadline) */
 } dpa_request;
 
 /* A finished request. Arrays are host memory owned by the server until
@@ -333,7 +381,7 @@ typedef struct dpa_request {
 typedef struct dpa_response {
   uint64_t       id;
   void*          user;
-  int32_t        status;
+  int32_t        status;        /* DPA_OK, DPA_ERROR_TIMEOUT or DPA_ERROR_CANCELLED */
   uint64_t       count;
   const float*   positions;
   const uint64_t* remaining;
@@ -373,6 +421,10 @@ int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_s
 int dpa_server_add_field(dpa_server* server, const dpa_field* field, int32_t* field_id);
 /* Queues a request; DPA_ERROR_OUT_OF_MEMORY when it could never fit the arenas. */
 int dpa_server_submit(dpa_server* server, const dpa_request* request, uint64_t* id);
+/* Asks the server to drop a queued or running request; it comes back through
+ * dpa_server_poll with status DPA_ERROR_CANCELLED (or its normal result if it
+ * finished first). DPA_ERROR_INVALID_ARGUMENT for an unknown or returned id. */
+int dpa_server_cancel(dpa_server* server, uint64_t id);
 /* Takes one finished request (*got = 1), waiting up to wait_ms for one. */
 int dpa_server_poll(dpa_server* server, int32_t wait_ms, dpa_response* out, int32_t* got);
 int dpa_server_release(dpa_server* server, uint64_t id);

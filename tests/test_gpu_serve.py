@@ -182,3 +182,82 @@ def test_server_takes_memoryless_steppers_and_refuses_the_others(ctx, resident):
     want = alone(ctx, field, pos, 80, "runge_kutta_cash_karp_54", 0.02, True)
     np.testing.assert_array_equal(res.positions, want.inactive_particles.position)
     np.testing.assert_array_equal(res.vertices, want.integral_curves[0].vertices)
+
+
+def test_deadlines_and_cancels_drop_requests_and_spare_the_rest(ctx, resident):
+    """Failure handling on the host: a running request past its deadline, a
+    waiting request past its deadline and a cancelled request come back with
+    DPA_ERROR_TIMEOUT / DPA_ERROR_CANCELLED between ticks (no kernel waits
+    on the host), while the other requests of the mix finish bit-exact with
+    their results alone. Short tick budgets keep the long requests in flight
+    across many ticks."""
+    grid, field = resident["noise"]
+    offset, size = seeds.seed_box(grid)
+    box = ([0.0] * 3, [float(s - 1) for s in grid.shape])
+    long_pos = seeds.generate_random(offset, size, 20000, 0, aabb=box, seed=61).position
+    small = [seeds.generate_random(offset, size, 300 + 50 * i, 0, aabb=box, seed=70 + i).position
+             for i in range(4)]
+    with Server(ctx, particle_capacity=30000, vertex_capacity=0, steps_per_tick=8,
+                max_requests=16, max_bypass_ms=5000) as server:
+        fid = server.add_field(field)
+        # Runs (many ticks of 8 steps) past its 30 ms deadline.
+        timed_out = server.submit(fid, long_pos, 200000, step_size=0.01, deadline_ms=30)
+        # No room while the long request runs; its deadline passes in the queue.
+        waiting = server.submit(fid, long_pos[:15000], 100, deadline_ms=10)
+        cancelled = server.submit(fid, small[0], 10_000_000, step_size=0.001)
+        keep = [server.submit(fid, s, 150) for s in small[1:]]
+        time.sleep(0.05)
+        assert server.cancel(cancelled)
+        assert not server.cancel(123456)
+        results = {}
+        while len(results) < 3 + len(keep):
+            res = server.poll(wait_ms=5000)
+            assert res is not None, server.stats()
+            results[res.id] = res
+        assert not server.cancel(keep[0])  # already returned
+    r = results[timed_out]
+    assert r.status == 7  # DPA_ERROR_TIMEOUT, dropped while running
+    assert r.positions.shape == (20000, 3)
+    assert (r.termination == 4).any() and r.particle_steps > 0
+    assert r.vertices is None and r.ftle is None
+    assert results[waiting].status == 7 and results[waiting].positions.shape == (0, 3)
+    assert results[cancelled].status == 8  # DPA_ERROR_CANCELLED
+    for rid, s in zip(keep, small[1:]):
+        assert results[rid].status == 0
+        want = alone(ctx, field, s, 150, "runge_kutta_4", 0.25, False)
+        np.testing.assert_array_equal(results[rid].positions, want.inactive_particles.position)
+        np.testing.assert_array_equal(results[rid].termination,
+                                      want.inactive_particles.termination)
+
+
+def test_small_requests_pass_a_large_one_that_waits_for_room(ctx, resident):
+    """Admission scans the queue: while a large request waits for slots, the
+    small requests behind it that fit start (and finish) before it, and each
+    result is the same as alone."""
+    grid, field = resident["noise"]
+    offset, size = seeds.seed_box(grid)
+    box = ([0.0] * 3, [float(s - 1) for s in grid.shape])
+    big = seeds.generate_random(offset, size, 12000, 0, aabb=box, seed=81).position
+    small = [seeds.generate_random(offset, size, 200, 0, aabb=box, seed=90 + i).position
+             for i in range(3)]
+    with Server(ctx, particle_capacity=20000, vertex_capacity=0, steps_per_tick=8,
+                max_requests=16, small_request_seeds=1000, reserved_percent=10,
+                max_bypass_ms=10000) as server:
+        fid = server.add_field(field)
+        first = server.submit(fid, big, 3000, step_size=0.01)   # runs
+        second = server.submit(fid, big, 300, step_size=0.01)   # no room: waits
+        smalls = [server.submit(fid, s, 100) for s in small]    # pass it
+        order = []
+        results = {}
+        while len(results) < 2 + len(smalls):
+            res = server.poll(wait_ms=5000)
+            assert res is not None, server.stats()
+            results[res.id] = res
+            order.append(res.id)
+    assert order.index(second) > max(order.index(s) for s in smalls)
+    assert all(results[s].admitted < results[second].admitted for s in smalls)
+    for rid, s in zip(smalls, small):
+        want = alone(ctx, field, s, 100, "runge_kutta_4", 0.25, False)
+        np.testing.assert_array_equal(results[rid].positions, want.inactive_particles.position)
+    want = alone(ctx, field, big, 300, "runge_kutta_4", 0.01, False)
+    np.testing.assert_array_equal(results[second].positions, want.inactive_particles.position)

@@ -104,3 +104,88 @@ def test_range_allocator_is_first_fit_and_merges_free_ranges(tmp_path):
                    check=True)
     run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert run.returncode == 0 and run.stdout.strip() == "ok", run.stdout + run.stderr
+
+
+ADMISSION_DRIVER = r"""
+#include <cstdio>
+#include <deque>
+#include <vector>
+#include "admission.hpp"
+#include "range_allocator.hpp"
+
+struct req { int id; uint64_t seeds; double queued; };
+
+// Runs one admission scan at time `now` over `q` with `free_slots` free (of
+// `capacity`, allocated first fit) and returns the admitted ids in order.
+static std::vector<int> scan(std::deque<req>& q, const dpa::admission_config& c, uint64_t used,
+                             double now, int counters = 1000) {
+  dpa::range_allocator slots(c.slot_capacity);
+  uint64_t at = 0;
+  if (used) slots.allocate(used, &at);
+  std::vector<int> got;
+  dpa::admit_waiting(
+      q, c, used, [](const req& r) { return r.seeds; }, [&](const req& r) { return now - r.queued; },
+      [&](const req& r) { uint64_t o; return slots.allocate(r.seeds, &o); },
+      [&](req& r) { got.push_back(r.id); --counters; }, [&] { return counters > 0; });
+  return got;
+}
+
+static int fail(const char* what) { std::printf("%s\n", what); return 1; }
+
+int main() {
+  dpa::admission_config c;
+  c.slot_capacity = 1000;
+  c.small_seeds = 10;
+  c.reserved_slots = 100;
+  c.max_bypass_seconds = 1.0;
+  {  // A small request passes a large one that has no room yet.
+    std::deque<req> q = {{1, 600, 0.0}, {2, 5, 0.1}, {3, 8, 0.2}};
+    const auto got = scan(q, c, 500, 0.5);
+    if (got != std::vector<int>({2, 3}) || q.size() != 1 || q.front().id != 1)
+      return fail("small requests did not pass the blocked large one");
+  }
+  {  // Large requests stop at capacity - reserved; small ones use the reserve.
+    std::deque<req> q = {{1, 400, 0.0}, {2, 400, 0.0}, {3, 100, 0.0}, {4, 10, 0.0}, {5, 10, 0.0}};
+    const auto got = scan(q, c, 0, 0.5);
+    // Large requests fill up to 900 of the 1000 slots; the small ones then
+    // take reserved slots.
+    if (got != std::vector<int>({1, 2, 3, 4, 5})) return fail("fill up to the reserve");
+    std::deque<req> q2 = {{6, 50, 0.0}, {7, 10, 0.0}};
+    const auto got2 = scan(q2, c, 880, 0.5);
+    if (got2 != std::vector<int>({7})) return fail("a large request took reserved slots");
+  }
+  {  // Once the oldest has waited max_bypass_seconds, nothing passes it...
+    std::deque<req> q = {{1, 600, 0.0}, {2, 5, 0.1}};
+    const auto got = scan(q, c, 500, 1.5);
+    if (!got.empty() || q.size() != 2) return fail("a request passed the overdue head");
+  }
+  {  // ...and it may then take reserved slots.
+    std::deque<req> q = {{1, 950, 0.0}, {2, 5, 0.1}};
+    const auto got = scan(q, c, 0, 1.5);
+    if (got != std::vector<int>({1, 2})) return fail("the overdue head could not use the reserve");
+  }
+  {  // Admission stops when no request counter is free.
+    std::deque<req> q = {{1, 5, 0.0}, {2, 5, 0.0}, {3, 5, 0.0}};
+    const auto got = scan(q, c, 0, 0.0, 2);
+    if (got != std::vector<int>({1, 2}) || q.size() != 1) return fail("counter limit ignored");
+  }
+  {  // A head that is not overdue may be passed, and a later one blocks nothing.
+    std::deque<req> q = {{1, 600, 0.9}, {2, 700, 0.0}, {3, 5, 0.95}};
+    const auto got = scan(q, c, 500, 1.2);
+    if (got != std::vector<int>({3})) return fail("only the oldest may stop the scan");
+  }
+  std::puts("ok");
+  return 0;
+}
+"""
+
+
+@pytest.mark.skipif(shutil.which("g++") is None, reason="no C++ compiler")
+def test_admission_passes_small_requests_within_the_reserve_and_bypass_limits(tmp_path):
+    src = tmp_path / "admission.cpp"
+    exe = tmp_path / "admission"
+    src.write_text(ADMISSION_DRIVER)
+    subprocess.run(["g++", "-std=c++17", "-O1", "-Wall", "-I", str(CSRC), str(src), "-o", str(exe)],
+                   check=True)
+    run = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert run.returncode == 0 and run.stdout.strip() == "ok", run.stdout + run.stderr
