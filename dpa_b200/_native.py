@@ -167,6 +167,7 @@ SIGNATURES = {
     "dpa_context_stream": (C.c_void_p, [_P]),
     "dpa_context_synchronize": (C.c_int, [_P]),
     "dpa_context_set_staging_limit": (C.c_int, [_P, C.c_uint64]),
+    "dpa_context_set_host_chunk_limit": (C.c_int, [_P, C.c_uint64]),
     "dpa_context_set_profiling": (C.c_int, [_P, C.c_int32]),
     "dpa_context_last_timing": (C.c_int, [_P, _F32P, _F32P]),
     "dpa_context_last_emit_timing": (C.c_int, [_P, _F32P]),
@@ -182,6 +183,8 @@ SIGNATURES = {
     "dpa_field_create_unsteady": (C.c_int, [_P, _P, _U64P, C.c_uint32, _F32P, _F32P, C.c_float,
                                             C.c_float, C.c_int32, C.POINTER(C.c_void_p)]),
     "dpa_field_time_info": (C.c_int, [_P, C.POINTER(C.c_uint32), _F32P, _F32P]),
+    "dpa_field_locate_mode": (C.c_int, [_P, C.POINTER(C.c_int32)]),
+    "dpa_context_set_ieee_division": (C.c_int, [_P, C.c_int32]),
     "dpa_advect_round": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _P, _P, _P,
                                    CURVE_SINK, _P]),
     "dpa_advect_device": (C.c_int, [_P, _P, C.POINTER(AdvectOptions), C.c_uint64, _P, _P, _P, _P]),

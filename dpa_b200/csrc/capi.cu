@@ -147,7 +147,8 @@ int record_piece(dpa_context* ctx, const dpa_field* field, const dpa_advect_opti
   cudaStream_t s = ctx->stream;
   const uint64_t n = end - begin;
   // Raw (unpruned) vertex offsets: remaining + 2 slots per particle.
-  std::vector<uint64_t> offsets(n);
+  DPA_TRY_CUDA(ctx, ctx->host_offsets.reserve(n * 8));
+  uint64_t* offsets = ctx->host_offsets.as<uint64_t>();
   uint64_t raw_total = 0;
   for (uint64_t i = 0; i < n; ++i) {
     offsets[i] = raw_total;
@@ -162,8 +163,10 @@ int record_piece(dpa_context* ctx, const dpa_field* field, const dpa_advect_opti
   DPA_TRY_CUDA(ctx, ctx->segment_offsets.reserve(n * 8));
   DPA_TRY_CUDA(ctx, ctx->totals.reserve(32));
   DPA_TRY_CUDA(ctx, ctx->host_totals.reserve(32));
-  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->raw_offsets.ptr, offsets.data(), n * 8,
-                                    cudaMemcpyHostToDevice, s));
+  // The pinned offsets of the previous piece are free: its copies finished
+  // before the previous piece returned.
+  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->raw_offsets.ptr, offsets, n * 8, cudaMemcpyHostToDevice,
+                                    s));
 
   float* positions = ctx->positions.as<float>() + 3 * begin;
   uint64_t* remaining = ctx->remaining.as<uint64_t>() + begin;
@@ -223,9 +226,6 @@ int record_piece(dpa_context* ctx, const dpa_field* field, const dpa_advect_opti
   DPA_TRY_CUDA(ctx, ctx->out_vertices.reserve(piece_vertices * 12));
   DPA_TRY_CUDA(ctx, ctx->out_colors.reserve(piece_vertices * 4));
   DPA_TRY_CUDA(ctx, ctx->out_indices.reserve(piece_indices * index_bytes));
-  DPA_TRY_CUDA(ctx, ctx->host_vertices.reserve(piece_vertices * 12));
-  DPA_TRY_CUDA(ctx, ctx->host_colors.reserve(piece_vertices * 4));
-  DPA_TRY_CUDA(ctx, ctx->host_indices.reserve(piece_indices * index_bytes));
 
   dpa::EmitArgs e{};
   e.count = n;
@@ -242,13 +242,75 @@ int record_piece(dpa_context* ctx, const dpa_field* field, const dpa_advect_opti
   DPA_TRY_CUDA(ctx, dpa::launch_emit(e, o->index64 != 0, o->colors != 0, s));
   ctx->launches += 1;
   if (ctx->profiling) DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->events[4], s));
-  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->host_vertices.ptr, ctx->out_vertices.ptr,
-                                    piece_vertices * 12, cudaMemcpyDeviceToHost, s));
-  if (o->colors)
-    DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->host_colors.ptr, ctx->out_colors.ptr,
-                                      piece_vertices * 4, cudaMemcpyDeviceToHost, s));
-  DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->host_indices.ptr, ctx->out_indices.ptr,
-                                    piece_indices * index_bytes, cudaMemcpyDeviceToHost, s));
+
+  // The piece's curve crosses to the host in chunks through two pinned
+  // halves, so that chunk j + 1 copies while the sink takes chunk j and the
+  // pinned memory stays bounded (dpa_context_set_host_chunk_limit).
+  if (sink) {
+    const uint64_t cap_v = std::max<uint64_t>(ctx->host_chunk_bytes / 16, 1);
+    const uint64_t cap_i = std::max<uint64_t>(ctx->host_chunk_bytes / index_bytes, 2) & ~1ull;
+    const uint64_t chunks = std::max<uint64_t>(
+        {1, (piece_vertices + cap_v - 1) / cap_v, (piece_indices + cap_i - 1) / cap_i});
+    const uint64_t half_v = std::min(piece_vertices, cap_v);
+    const uint64_t half_i = std::min(piece_indices, cap_i);
+    DPA_TRY_CUDA(ctx, ctx->host_vertices.reserve(2 * half_v * 12));
+    DPA_TRY_CUDA(ctx, ctx->host_colors.reserve(2 * half_v * 4));
+    DPA_TRY_CUDA(ctx, ctx->host_indices.reserve(2 * half_i * index_bytes));
+    for (cudaEvent_t& ev : ctx->chunk_events)
+      if (!ev) DPA_TRY_CUDA(ctx, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    auto span = [](uint64_t j, uint64_t cap, uint64_t total, uint64_t* first, uint64_t* count) {
+      *first = std::min(j * cap, total);
+      *count = std::min(cap, total - *first);
+    };
+    auto issue = [&](uint64_t j) -> int {
+      const uint64_t h = j & 1;
+      uint64_t v0, vn, i0, in;
+      span(j, cap_v, piece_vertices, &v0, &vn);
+      span(j, cap_i, piece_indices, &i0, &in);
+      if (vn) {
+        DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->host_vertices.as<float>() + 3 * h * half_v,
+                                          ctx->out_vertices.as<float>() + 3 * v0, vn * 12,
+                                          cudaMemcpyDeviceToHost, s));
+        if (o->colors)
+          DPA_TRY_CUDA(ctx, cudaMemcpyAsync(ctx->host_colors.as<float>() + h * half_v,
+                                            ctx->out_colors.as<float>() + v0, vn * 4,
+                                            cudaMemcpyDeviceToHost, s));
+      }
+      if (in)
+        DPA_TRY_CUDA(ctx, cudaMemcpyAsync(
+                              ctx->host_indices.as<char>() + h * half_i * index_bytes,
+                              ctx->out_indices.as<char>() + i0 * index_bytes, in * index_bytes,
+                              cudaMemcpyDeviceToHost, s));
+      DPA_TRY_CUDA(ctx, cudaEventRecord(ctx->chunk_events[h], s));
+      return DPA_OK;
+    };
+    int st = issue(0);
+    if (st != DPA_OK) return st;
+    for (uint64_t j = 0; j < chunks; ++j) {
+      if (j + 1 < chunks) {
+        st = issue(j + 1);  // into the half whose chunk the sink has returned
+        if (st != DPA_OK) return st;
+      }
+      const uint64_t h = j & 1;
+      DPA_TRY_CUDA(ctx, cudaEventSynchronize(ctx->chunk_events[h]));
+      uint64_t v0, vn, i0, in;
+      span(j, cap_v, piece_vertices, &v0, &vn);
+      span(j, cap_i, piece_indices, &i0, &in);
+      dpa_curve_chunk c{};
+      c.vertex_offset = *round_vertices + v0;
+      c.vertex_count = vn;
+      c.vertices = ctx->host_vertices.as<float>() + 3 * h * half_v;
+      c.colors = o->colors ? ctx->host_colors.as<float>() + h * half_v : nullptr;
+      c.index_offset = *round_indices + i0;
+      c.index_count = in;
+      c.indices = ctx->host_indices.as<char>() + h * half_i * index_bytes;
+      c.last = (final_piece && j + 1 == chunks) ? 1 : 0;
+      if (sink(user, &c) != 0) {
+        cudaStreamSynchronize(s);  // no copy may still target the halves
+        return fail(ctx, DPA_ERROR_SINK, "curve sink aborted the round");
+      }
+    }
+  }
   DPA_TRY_CUDA(ctx, cudaStreamSynchronize(s));
   if (ctx->profiling) {
     float order_ms = 0.0f, advect_ms = 0.0f, emit_ms = 0.0f;
@@ -258,19 +320,6 @@ int record_piece(dpa_context* ctx, const dpa_field* field, const dpa_advect_opti
     ctx->round_order_ms += order_ms;
     ctx->round_advect_ms += advect_ms;
     ctx->round_emit_ms += emit_ms;
-  }
-
-  if (sink) {
-    dpa_curve_chunk c{};
-    c.vertex_offset = *round_vertices;
-    c.vertex_count = piece_vertices;
-    c.vertices = ctx->host_vertices.as<float>();
-    c.colors = o->colors ? ctx->host_colors.as<float>() : nullptr;
-    c.index_offset = *round_indices;
-    c.index_count = piece_indices;
-    c.indices = ctx->host_indices.ptr;
-    c.last = final_piece ? 1 : 0;
-    if (sink(user, &c) != 0) return fail(ctx, DPA_ERROR_SINK, "curve sink aborted the round");
   }
   *round_vertices += piece_vertices;
   *round_indices += piece_indices;
@@ -322,6 +371,8 @@ int dpa_context_destroy(dpa_context* ctx) {
   ctx->release_all();
   for (cudaEvent_t e : ctx->events)
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : ctx->chunk_events)
+    if (e) cudaEventDestroy(e);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return DPA_OK;
@@ -345,6 +396,13 @@ int dpa_context_set_staging_limit(dpa_context* ctx, uint64_t bytes) {
   if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
   if (bytes < 4096) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "staging limit below 4 KiB");
   ctx->staging_limit = bytes;
+  return DPA_OK;
+}
+
+int dpa_context_set_host_chunk_limit(dpa_context* ctx, uint64_t bytes) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  if (bytes < 4096) return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "host chunk limit below 4 KiB");
+  ctx->host_chunk_bytes = bytes;
   return DPA_OK;
 }
 
@@ -568,7 +626,9 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
     v.stride1 = uint32_t(shape[2]);
     v.storage = storage;
     v.locate = dpa::kLocatePow2;
-    if (!pow2) {
+    if (!pow2 && ctx->ieee_division) {
+      v.locate = dpa::kLocateDivide;
+    } else if (!pow2) {
       bool exact = true;
       for (int i = 0; i < 3 && exact; ++i) {
         const int st = reciprocal_divides_exactly(ctx, spacing[i], &exact);
@@ -589,7 +649,7 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
     v.time_spacing = slices > 1 ? time_spacing : 1.0f;
     v.time_reciprocal = 1.0f / v.time_spacing;
     v.time_fast = 0;
-    if (slices > 1) {
+    if (slices > 1 && !ctx->ieee_division) {
       bool exact = false;
       const int st = reciprocal_divides_exactly(ctx, v.time_spacing, &exact);
       if (st != DPA_OK) {
@@ -625,6 +685,18 @@ int dpa_field_create_unsteady(dpa_context* ctx, const float* xyzv, const uint64_
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "a time-varying field needs 2 or more slices");
   return create_field(ctx, xyzv, false, shape, offset, spacing, storage, out, slices, time_origin,
                       time_spacing);
+}
+
+int dpa_context_set_ieee_division(dpa_context* ctx, int32_t enabled) {
+  if (!ctx) return DPA_ERROR_INVALID_ARGUMENT;
+  ctx->ieee_division = enabled != 0;
+  return DPA_OK;
+}
+
+int dpa_field_locate_mode(const dpa_field* field, int32_t* mode) {
+  if (!field || !mode) return DPA_ERROR_INVALID_ARGUMENT;
+  *mode = field->view.locate;
+  return DPA_OK;
 }
 
 int dpa_field_time_info(const dpa_field* field, uint32_t* slices, float* time_origin,

@@ -111,6 +111,9 @@ struct dpa_context {
   cudaStream_t stream = nullptr;
   std::string error;
   uint64_t staging_limit = 1ull << 30;
+  uint64_t host_chunk_bytes = 256ull << 20;  // per pinned half (vertices + colors; indices)
+  cudaEvent_t chunk_events[2] = {nullptr, nullptr};
+  bool ieee_division = false;  // fields created now divide by __fdiv_rn only
 
   DeviceBuffer positions, remaining, remaining_in, termination;
   dpa_launch_scratch scratch;
@@ -126,7 +129,7 @@ struct dpa_context {
   DeviceBuffer raw, raw_offsets, raw_counts, kept_vertices, kept_segments;
   DeviceBuffer wide, vertex_offsets, segment_offsets, scan_temp, totals;
   DeviceBuffer out_vertices, out_colors, out_indices;
-  PinnedBuffer host_vertices, host_colors, host_indices, host_totals;
+  PinnedBuffer host_vertices, host_colors, host_indices, host_totals, host_offsets;
   DeviceBuffer ftle_winners, ftle_flow, ftle_out, ftle_original, ftle_final;
 
   void release_all() {
@@ -138,7 +141,8 @@ struct dpa_context {
                          &out_indices, &ftle_winners, &ftle_flow, &ftle_out, &ftle_original,
                          &ftle_final};
     for (DeviceBuffer* b : d) b->release();
-    PinnedBuffer* h[] = {&host_vertices, &host_colors, &host_indices, &host_totals};
+    PinnedBuffer* h[] = {&host_vertices, &host_colors, &host_indices, &host_totals,
+                         &host_offsets};
     for (PinnedBuffer* b : h) b->release();
   }
 };

@@ -108,7 +108,9 @@ typedef struct dpa_advect_options {
                            calls without recording only) */
 } dpa_advect_options;
 
-/* One piece of a round's curve, delivered in order. The round's curve is the
+/* One chunk of a round's curve, delivered in order (a round arrives in one or
+ * more chunks; vertex and index ranges each continue where the previous chunk
+ * ended). The round's curve is the
  * reference's integral_curve after advect, prune_integral_curves,
  * index_generator::generate and color_generator::generate_from_angular_velocities
  * (particle_advector.cpp:402-408, index_generator.cpp:10-39,
@@ -151,6 +153,12 @@ int dpa_context_synchronize(dpa_context* ctx);
 /* Upper bound on the device bytes a recording round may stage at once; larger
  * rounds are processed in pieces (default 1 GiB). */
 int dpa_context_set_staging_limit(dpa_context* ctx, uint64_t bytes);
+
+/* Upper bound on the curve bytes one sink chunk carries (default 256 MiB of
+ * vertices and colors, and as many bytes of indices). A piece's curve crosses
+ * to the host through two pinned buffers of this size, the next chunk copying
+ * while the sink takes the current one. */
+int dpa_context_set_host_chunk_limit(dpa_context* ctx, uint64_t bytes);
 
 /* Instrumentation, the counterpart of the reference's per-round timers
  * (pipeline.cpp:98-145, benchmark.hpp:152-158). With profiling on, every
@@ -220,6 +228,18 @@ int dpa_field_create_unsteady(dpa_context* ctx, const float* xyzv, const uint64_
                               uint32_t slices, const float offset[3], const float spacing[3],
                               float time_origin, float time_spacing, int32_t storage,
                               dpa_field** out);
+
+/* How the field's kernels divide a position by the spacing: 2 = power-of-two
+ * spacings (one FMA of exact scaled values), 1 = Markstein's division by the
+ * rounded reciprocal (one multiply and two FMAs), used only for spacings for
+ * which it was checked on the device, at field creation, to give IEEE
+ * division's bits for every float dividend, 0 = IEEE division. All three give
+ * the reference's rounded quotient. */
+int dpa_field_locate_mode(const dpa_field* field, int32_t* mode);
+
+/* Fields created on this context from now on use IEEE division (mode 0)
+ * whatever their spacing, when enabled (for comparison; off by default). */
+int dpa_context_set_ieee_division(dpa_context* ctx, int32_t enabled);
 
 /* slices = 1 (and zero times) for a steady field. */
 int dpa_field_time_info(const dpa_field* field, uint32_t* slices, float* time_origin,

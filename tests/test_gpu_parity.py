@@ -23,7 +23,7 @@ def _seeds_in_box(grid, count, seed, box=None):
 
 
 def compare(ctx, oracle, grid, positions, iterations, integrator, step, ppr, record,
-            storage="f32", index64=False, morton=True, staging=None):
+            storage="f32", index64=False, morton=True, staging=None, host_chunk=None):
     """Runs the GPU rounds and the oracle rounds on the same input."""
     oracle_data = grid.data
     if storage == "f16":
@@ -37,12 +37,16 @@ def compare(ctx, oracle, grid, positions, iterations, integrator, step, ppr, rec
                                              index64)
     if staging:
         ctx.set_staging_limit(staging)
+    if host_chunk:
+        ctx.check(ctx._lib.dpa_context_set_host_chunk_limit(ctx.handle, host_chunk))
     field = ctx.field(grid, storage)
     adv = ParticleAdvector(ctx, ppr, "none", integrator, step, False, record,
                            use_64_bit_indices=index64, morton_order=morton)
     got = adv.advect(field, Particles.create(positions, rem))
     if staging:
         ctx.set_staging_limit(1 << 30)
+    if host_chunk:
+        ctx.check(ctx._lib.dpa_context_set_host_chunk_limit(ctx.handle, 256 << 20))
     np.testing.assert_array_equal(got.inactive_particles.termination, want.termination)
     np.testing.assert_array_equal(got.inactive_particles.remaining_iterations, want.remaining)
     np.testing.assert_array_equal(got.inactive_particles.position, want.positions)
@@ -90,6 +94,17 @@ def test_u64_indices_and_small_staging_pieces(ctx, oracle):
             staging=12 * 122 * 50)
     compare(ctx, oracle, grid, pos, 120, "runge_kutta_4", 0.02, 777, True, index64=False,
             staging=12 * 122 * 7)
+
+
+@pytest.mark.parametrize("index64", [False, True])
+def test_curve_chunks_through_small_pinned_halves(ctx, oracle, index64):
+    # A host chunk limit of 4 KiB splits every piece's curve into many chunks
+    # (vertices and indices split at different places), copied through the
+    # two pinned halves while the sink takes the previous chunk.
+    grid = fields.abc(32)
+    pos = _seeds_in_box(grid, 600, 12, ([0, 0, 0], [2 * math.pi] * 3))
+    compare(ctx, oracle, grid, pos, 150, "runge_kutta_4", 0.02, 600, True, index64=index64,
+            staging=12 * 152 * 200, host_chunk=4096)
 
 
 def test_curl_noise_power_of_two_spacing_end_positions(ctx, oracle):
@@ -250,3 +265,79 @@ def test_degenerate_and_anisotropic_grids(ctx, oracle):
         hi = lo + np.asarray(spacing, np.float32) * (np.asarray(data.shape[:3]) - 1)
         pos = (lo + rng.random((300, 3)) * (hi - lo) * 1.02 - 0.01 * (hi - lo)).astype(np.float32)
         compare(ctx, oracle, grid, pos, 40, "runge_kutta_4", 0.05, 300, True)
+
+
+def _locate_mode(ctx, field):
+    import ctypes as C
+    mode = C.c_int32()
+    ctx.check(ctx._lib.dpa_field_locate_mode(field.handle, C.byref(mode)))
+    return mode.value
+
+
+@pytest.mark.parametrize("spacing", [2 * math.pi / 63, 0.7, 1.0 / 3.0])
+def test_reciprocal_division_matches_ieee_division_and_oracle(ctx, oracle, spacing):
+    """Non-power-of-two spacings divide by the rounded reciprocal once the
+    device has checked it against IEEE division for every float dividend;
+    results are bit-exact with the IEEE-division kernels and with the oracle."""
+    data = fields.curl_noise(40, 3.0, 13).data
+    grid = dpa_b200.RegularGrid.from_data(data, (spacing, spacing, spacing), (0.25, -0.5, 0.0))
+    pos = _seeds_in_box(grid, 3000, 14)
+    step = float(np.float32(0.3 * spacing))
+    og = oracle.OracleGrid(grid.data, grid.spacing, grid.offset)
+    rem = np.full(pos.shape[0], 250, np.uint64)
+    want = oracle.advect_round(og, "runge_kutta_4", step, pos, rem, record=True)
+    modes = []
+    try:
+        for ieee in (0, 1):
+            ctx.check(ctx._lib.dpa_context_set_ieee_division(ctx.handle, ieee))
+            field = ctx.field(grid)
+            modes.append(_locate_mode(ctx, field))
+            adv = ParticleAdvector(ctx, pos.shape[0], "none", "runge_kutta_4", step, False, True)
+            got = adv.advect(field, Particles.create(pos, rem))
+            field.close()
+            np.testing.assert_array_equal(got.inactive_particles.position, want.positions)
+            np.testing.assert_array_equal(got.inactive_particles.termination, want.termination)
+            np.testing.assert_array_equal(got.integral_curves[0].vertices, want.vertices)
+            np.testing.assert_array_equal(got.integral_curves[0].indices, want.indices)
+    finally:
+        ctx.check(ctx._lib.dpa_context_set_ieee_division(ctx.handle, 0))
+    assert modes[1] == 0 and modes[0] in (0, 1), modes
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16"])
+@pytest.mark.parametrize("integrator", ["runge_kutta_4", "runge_kutta_cash_karp_54"])
+def test_two_particles_per_lane_and_block_sizes_match_oracle(ctx, oracle, storage, integrator):
+    """Every launch shape the autotuner may pick -- 64 to 256 threads per
+    block, one or two particles per lane -- gives the oracle's results bit
+    for bit, including step budgets resumed over several calls."""
+    import ctypes as C
+    import torch
+    from dpa_b200 import _native as N
+    grid = fields.curl_noise(48, 3.0, 15)
+    pos = _seeds_in_box(grid, 5000, 16)
+    data = grid.data if storage == "f32" else grid.data.astype(np.float16).astype(np.float32)
+    og = oracle.OracleGrid(data, grid.spacing, grid.offset)
+    want = oracle.advect_round(og, integrator, 0.25, pos, np.full(5000, 300, np.uint64))
+    field = ctx.field(grid, storage)
+    saved = N.Tuning()
+    ctx.check(ctx._lib.dpa_context_get_tuning(ctx.handle, C.byref(saved)))
+    try:
+        for block, ppt, budget in ((256, 2, 0), (64, 2, 0), (128, 1, 0), (64, 2, 77), (96, 2, 0)):
+            t = N.Tuning(16, 0, 64, 0.0, block, ppt)
+            ctx.check(ctx._lib.dpa_context_set_tuning(ctx.handle, C.byref(t)))
+            p = torch.from_numpy(pos).cuda()
+            r = torch.full((5000,), 300, dtype=torch.int64, device="cuda")
+            term = torch.zeros(5000, dtype=torch.uint8, device="cuda")
+            opts = N.AdvectOptions(N.INTEGRATORS[integrator], 0.25, 0, 0, 0, 1, budget)
+            for _ in range(300 // budget + 1 if budget else 1):
+                ctx.check(ctx._lib.dpa_advect_device(ctx.handle, field.handle, C.byref(opts),
+                                                     5000, C.c_void_p(p.data_ptr()),
+                                                     C.c_void_p(r.data_ptr()),
+                                                     C.c_void_p(term.data_ptr()), None))
+            ctx.synchronize()
+            np.testing.assert_array_equal(p.cpu().numpy(), want.positions)
+            np.testing.assert_array_equal(r.cpu().numpy().astype(np.uint64), want.remaining)
+            np.testing.assert_array_equal(term.cpu().numpy(), want.termination)
+    finally:
+        ctx.check(ctx._lib.dpa_context_set_tuning(ctx.handle, C.byref(saved)))
+        field.close()
