@@ -91,6 +91,7 @@ class ServerOptions(C.Structure):
         ("small_request_seeds", C.c_uint64),
         ("reserved_percent", C.c_uint32),
         ("max_bypass_ms", C.c_uint32),
+        ("response_bytes", C.c_uint64),
     ]
 
 

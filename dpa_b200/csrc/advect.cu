@@ -168,19 +168,16 @@ __global__ void expand_ranges_kernel(const uint64_t* starts, const uint64_t* fir
 }
 
 // Counts the dividends a (every 32-bit pattern) for which
-// divide_by_reciprocal(a, h, y) and __fdiv_rn(a, h) differ in their bits.
-// Results that are both non-finite count as equal: either one places a
-// position outside the grid.
-__global__ void verify_division_kernel(float h, float y, unsigned int* mismatches) {
+// divide_by_reciprocal(a, h, y, yl) and __fdiv_rn(a, h) differ in their bits.
+__global__ void verify_division_kernel(float h, float y, float yl, unsigned int* mismatches) {
   const uint64_t stride = uint64_t(gridDim.x) * blockDim.x;
   unsigned int bad = 0;
   for (uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < (1ull << 32);
        i += stride) {
     const float a = __uint_as_float(uint32_t(i));
     const float want = __fdiv_rn(a, h);
-    const float got = divide_by_reciprocal(a, h, y);
-    const bool same = __float_as_uint(want) == __float_as_uint(got) ||
-                      (!isfinite(want) && !isfinite(got));
+    const float got = divide_by_reciprocal(a, h, y, yl);
+    const bool same = __float_as_uint(want) == __float_as_uint(got) || (isnan(want) && isnan(got));
     bad += same ? 0u : 1u;
   }
 #pragma unroll
@@ -239,10 +236,10 @@ cudaError_t launch_gather_probe(const float4* table, uint32_t mask, uint32_t sid
   return cudaGetLastError();
 }
 
-cudaError_t launch_verify_division(float h, float y, unsigned int* mismatches,
+cudaError_t launch_verify_division(float h, float y, float yl, unsigned int* mismatches,
                                    cudaStream_t stream) {
   DPA_CUDA_TRY(cudaMemsetAsync(mismatches, 0, sizeof(unsigned int), stream));
-  verify_division_kernel<<<148 * 8, 256, 0, stream>>>(h, y, mismatches);
+  verify_division_kernel<<<148 * 8, 256, 0, stream>>>(h, y, yl, mismatches);
   return cudaGetLastError();
 }
 

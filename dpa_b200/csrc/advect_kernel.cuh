@@ -54,8 +54,7 @@ constexpr int advect_min_blocks() {
 // counter per stretch (a stretch ends at 2^32 - 1 steps at the latest). The
 // kPPT slots of a lane step in lock-step, so one particle's corner gather is
 // in flight while the other's arithmetic issues. An empty slot holds a NaN
-// position: its step fails the grid test at once, touches no memory and is
-// never counted.
+// position and takes no steps.
 template <int kIntegrator, int kStorage, int kLocate, bool kRecord, bool kUnsteady, int kPPT>
 __global__ void __launch_bounds__(kAdvectBlock, advect_min_blocks<kIntegrator, kUnsteady, kPPT>())
 advect_kernel(const FieldView f, const AdvectArgs a) {
@@ -192,9 +191,12 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
       halt = halt || stop[j];
     }
     while (!__any_sync(kFull, halt)) {
+      // An empty slot does not step: its NaN position would send IEEE
+      // division into its slow path, which the whole warp would wait for.
 #pragma unroll
       for (int j = 0; j < kPPT; ++j)
-        r[j] = step<kIntegrator>(f, a.coefficients, sampler[j], p[j], t[j], history[j]);
+        r[j] = active[j] ? step<kIntegrator>(f, a.coefficients, sampler[j], p[j], t[j], history[j])
+                         : int(kStepOutOfBounds);
       halt = false;
 #pragma unroll
       for (int j = 0; j < kPPT; ++j) {

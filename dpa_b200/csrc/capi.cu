@@ -526,10 +526,18 @@ int dpa_integrator_from_name(const char* name, int32_t* integrator) {
   return DPA_ERROR_INVALID_ARGUMENT;
 }
 
-// Whether dividing by h through its rounded reciprocal (Markstein's division,
-// divide_by_reciprocal) gives IEEE division's bits for every float dividend:
-// checked once per divisor and process on the device, over all 2^32 bit
-// patterns (a few milliseconds), and remembered.
+// The reciprocal of h split into two floats: hi = RN(1 / h), lo =
+// RN(1 / h - hi), with 1 / h taken in the host's extended precision.
+static void split_reciprocal(float h, float* hi, float* lo) {
+  const long double inv = 1.0L / static_cast<long double>(h);
+  *hi = static_cast<float>(inv);
+  *lo = static_cast<float>(inv - static_cast<long double>(*hi));
+}
+
+// Whether dividing by h through its split reciprocal (divide_by_reciprocal)
+// gives IEEE division's bits for every float dividend: checked once per
+// divisor and process on the device, over all 2^32 bit patterns (a few
+// milliseconds), and remembered.
 static int reciprocal_divides_exactly(dpa_context* ctx, float h, bool* exact) {
   static std::mutex lock;
   static std::map<uint32_t, bool> known;
@@ -545,7 +553,9 @@ static int reciprocal_divides_exactly(dpa_context* ctx, float h, bool* exact) {
   }
   DeviceBuffer counter;
   DPA_TRY_CUDA(ctx, counter.reserve(sizeof(unsigned int)));
-  DPA_TRY_CUDA(ctx, dpa::launch_verify_division(h, 1.0f / h, counter.as<unsigned int>(),
+  float hi = 0.0f, lo = 0.0f;
+  split_reciprocal(h, &hi, &lo);
+  DPA_TRY_CUDA(ctx, dpa::launch_verify_division(h, hi, lo, counter.as<unsigned int>(),
                                                 ctx->stream));
   unsigned int mismatches = 0;
   DPA_TRY_CUDA(ctx, cudaMemcpyAsync(&mismatches, counter.ptr, sizeof mismatches,
@@ -618,7 +628,10 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
       v.n[i] = int32_t(shape[i]);
       v.offset[i] = offset[i];
       v.spacing[i] = spacing[i];
-      v.reciprocal[i] = 1.0f / spacing[i];
+      float hi = 0.0f, lo = 0.0f;
+      split_reciprocal(spacing[i], &hi, &lo);
+      v.reciprocal[i] = hi;
+      v.reciprocal_lo[i] = lo;
       v.scaled_offset[i] = offset[i] * v.reciprocal[i];
       v.upper[i] = float(int64_t(shape[i]) - 1);
     }
@@ -647,7 +660,7 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
     v.slice_stride = int64_t(slice_nodes);
     v.time_origin = time_origin;
     v.time_spacing = slices > 1 ? time_spacing : 1.0f;
-    v.time_reciprocal = 1.0f / v.time_spacing;
+    split_reciprocal(v.time_spacing, &v.time_reciprocal, &v.time_reciprocal_lo);
     v.time_fast = 0;
     if (slices > 1 && !ctx->ieee_division) {
       bool exact = false;

@@ -26,10 +26,10 @@ constexpr float kZeroPrecision = 1e-5f;
 
 // How a kernel divides a position by the spacing (per field, every axis):
 //   kLocateDivide      IEEE division (__fdiv_rn);
-//   kLocateReciprocal  a / h as one product by y = RN(1 / h) and one FMA
-//                      correction (Markstein's division), used only for
-//                      divisors for which it was checked at field creation to
-//                      equal __fdiv_rn for every finite float a;
+//   kLocateReciprocal  a / h as one product and one FMA with the reciprocal
+//                      split in two floats (divide_by_reciprocal), used only
+//                      for divisors for which it was checked at field creation
+//                      to equal __fdiv_rn for every float a;
 //   kLocatePow2        power-of-two spacing: one FMA of the exact p / h and
 //                      offset / h, and fmod(p - offset, h) / h = q - floor(q).
 enum LocateMode : int { kLocateDivide = 0, kLocateReciprocal = 1, kLocatePow2 = 2 };
@@ -46,6 +46,7 @@ struct FieldView {
   float offset[3];
   float spacing[3];
   float reciprocal[3];     // RN(1 / spacing): exact for power-of-two spacings
+  float reciprocal_lo[3];  // RN(1 / spacing - reciprocal)
   float scaled_offset[3];  // offset / spacing, exact; used by kLocatePow2 only
   float upper[3];          // n - 1: inside iff 0 <= (p - offset) / h < n - 1
   int32_t storage;         // dpa_storage
@@ -59,26 +60,30 @@ struct FieldView {
   int64_t slice_stride;
   float time_origin;
   float time_spacing;
-  float time_reciprocal;   // RN(1 / time_spacing)
-  int32_t time_fast;       // time_reciprocal divides exactly (as kLocateReciprocal)
+  float time_reciprocal;     // RN(1 / time_spacing)
+  float time_reciprocal_lo;  // RN(1 / time_spacing - time_reciprocal)
+  int32_t time_fast;         // the time axis divides as kLocateReciprocal
   float time_upper;      // slices - 1: inside iff 0 <= (t - t0) / dt < slices - 1
 };
 
-// a / h with y = RN(1 / h): q0 = RN(a y), r = a - q0 h (exact, one FMA),
-// q = RN(q0 + r y). Markstein's division ("Computation of elementary functions
-// on the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990);
-// its result is used only for divisors verified to equal IEEE division for
-// every finite dividend (verify_reciprocal_division, emit.cu).
-__device__ __forceinline__ float divide_by_reciprocal(float a, float h, float y) {
-  const float q0 = __fmul_rn(a, y);
-  const float r = __fmaf_rn(-q0, h, a);
-  return __fmaf_rn(r, y, q0);
+// a / h by a known divisor: with y + yl = 1 / h split into two floats,
+// q = RN(a * y + RN(a * yl)), one product and one FMA (Brisebarre, Muller
+// and Raina, "Accelerating correctly rounded floating-point division when
+// the divisor is known in advance", IEEE Trans. Computers 53(8), 2004).
+// Dividends below 2^-64 or above 2^64 in magnitude (and NaN) take IEEE
+// division: there the products leave the normal range. Whether the result
+// equals IEEE division for every other dividend depends on the divisor; it
+// is used only for divisors checked exhaustively on the device
+// (verify_division_kernel, advect.cu).
+__device__ __forceinline__ float divide_by_reciprocal(float a, float h, float y, float yl) {
+  if (!(fabsf(a) >= 0x1p-64f && fabsf(a) <= 0x1p64f)) return __fdiv_rn(a, h);
+  return __fmaf_rn(a, y, __fmul_rn(a, yl));
 }
 
 template <int kLocate>
-__device__ __forceinline__ float divide_spacing(float a, float h, float y) {
+__device__ __forceinline__ float divide_spacing(float a, float h, float y, float yl) {
   if constexpr (kLocate == kLocateDivide) return __fdiv_rn(a, h);
-  else return divide_by_reciprocal(a, h, y);
+  else return divide_by_reciprocal(a, h, y, yl);
 }
 
 // Integrator id of the kernel instantiation shared by the reference's other

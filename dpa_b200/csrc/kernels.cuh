@@ -165,8 +165,8 @@ cudaError_t launch_gather_probe(const float4* table, uint32_t mask, uint32_t sid
                                 cudaStream_t stream);
 
 // Counts into *mismatches (zeroed first) the 32-bit dividends for which
-// divide_by_reciprocal(a, h, y) differs from IEEE division by h.
-cudaError_t launch_verify_division(float h, float y, unsigned int* mismatches,
+// divide_by_reciprocal(a, h, y, yl) differs from IEEE division by h.
+cudaError_t launch_verify_division(float h, float y, float yl, unsigned int* mismatches,
                                    cudaStream_t stream);
 
 // Field repack: XYZV float [n][3] -> 4-wide nodes in the given storage.

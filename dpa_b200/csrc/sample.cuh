@@ -90,14 +90,14 @@ struct Weights {
 // or N + 1 (only when a / h lies within half an ulp below N + 1, so that
 // fmod(a, h) >= h / 2). In both cases a - s * h is exactly representable, so
 // one FMA gives it exactly; adding h back in the N + 1 case is exact too.
-// Both divisions are IEEE-exact (kLocateDivide) or by the verified reciprocal
-// (kLocateReciprocal), which gives the same bits.
+// Both divisions are IEEE division (kLocateDivide) or by the verified
+// reciprocal pair (kLocateReciprocal), which gives the same bits.
 template <int kLocate>
-__device__ __forceinline__ float weight_general(float a, float s, float h, float y) {
+__device__ __forceinline__ float weight_general(float a, float s, float h, float y, float yl) {
   float r = fmaf(-s, h, a);
   if (r < 0.0f) r = __fadd_rn(r, h);
   if (r == 0.0f) r = copysignf(0.0f, a);
-  return divide_spacing<kLocate>(r, h, y);
+  return divide_spacing<kLocate>(r, h, y, yl);
 }
 
 // Locates p; node receives the index of the cell's first corner within its
@@ -120,9 +120,9 @@ __device__ __forceinline__ bool locate(const FieldView& f, const Position& p, ui
   } else {
     a0 = __fsub_rn(p.p0, f.offset[0]);
     a21 = sum2(p.p21, neg2(make_float2(f.offset[2], f.offset[1])));
-    q0 = divide_spacing<kLocate>(a0, f.spacing[0], f.reciprocal[0]);
-    q2 = divide_spacing<kLocate>(a21.x, f.spacing[2], f.reciprocal[2]);
-    q1 = divide_spacing<kLocate>(a21.y, f.spacing[1], f.reciprocal[1]);
+    q0 = divide_spacing<kLocate>(a0, f.spacing[0], f.reciprocal[0], f.reciprocal_lo[0]);
+    q2 = divide_spacing<kLocate>(a21.x, f.spacing[2], f.reciprocal[2], f.reciprocal_lo[2]);
+    q1 = divide_spacing<kLocate>(a21.y, f.spacing[1], f.reciprocal[1], f.reciprocal_lo[1]);
   }
   const bool inside = (q0 >= 0.0f) && (q0 < f.upper[0]) && (q1 >= 0.0f) && (q1 < f.upper[1]) &&
                       (q2 >= 0.0f) && (q2 < f.upper[2]);
@@ -132,9 +132,10 @@ __device__ __forceinline__ bool locate(const FieldView& f, const Position& p, ui
     const float2 d = sum2(make_float2(q2, q1), neg2(make_float2(s2, s1)));
     w.w21 = make_float2(copysignf(d.x, q2), copysignf(d.y, q1));
   } else {
-    w.w0 = weight_general<kLocate>(a0, s0, f.spacing[0], f.reciprocal[0]);
-    w.w21 = make_float2(weight_general<kLocate>(a21.x, s2, f.spacing[2], f.reciprocal[2]),
-                        weight_general<kLocate>(a21.y, s1, f.spacing[1], f.reciprocal[1]));
+    w.w0 = weight_general<kLocate>(a0, s0, f.spacing[0], f.reciprocal[0], f.reciprocal_lo[0]);
+    w.w21 = make_float2(
+        weight_general<kLocate>(a21.x, s2, f.spacing[2], f.reciprocal[2], f.reciprocal_lo[2]),
+        weight_general<kLocate>(a21.y, s1, f.spacing[1], f.reciprocal[1], f.reciprocal_lo[1]));
   }
   // Saturating conversions: outside the grid the value is never used.
   node = __float2uint_rz(s0) * f.stride0 + __float2uint_rz(s1) * f.stride1 + __float2uint_rz(s2);
@@ -309,15 +310,16 @@ struct CellSampler {
 __device__ __forceinline__ bool locate_time(const FieldView& f, float t, int64_t& slice_base,
                                             float& w) {
   const float a = __fsub_rn(t, f.time_origin);
-  const float y = f.time_reciprocal;
-  const float q = f.time_fast ? divide_by_reciprocal(a, f.time_spacing, y)
+  const float y = f.time_reciprocal, yl = f.time_reciprocal_lo;
+  const float q = f.time_fast ? divide_by_reciprocal(a, f.time_spacing, y, yl)
                               : __fdiv_rn(a, f.time_spacing);
   if (!(q >= 0.0f && q < f.time_upper)) return false;
   const float s = floorf(q);
   float r = fmaf(-s, f.time_spacing, a);
   if (r < 0.0f) r = __fadd_rn(r, f.time_spacing);
   if (r == 0.0f) r = copysignf(0.0f, a);
-  w = f.time_fast ? divide_by_reciprocal(r, f.time_spacing, y) : __fdiv_rn(r, f.time_spacing);
+  w = f.time_fast ? divide_by_reciprocal(r, f.time_spacing, y, yl)
+                   : __fdiv_rn(r, f.time_spacing);
   slice_base = int64_t(s) * f.slice_stride;
   return true;
 }

@@ -61,13 +61,18 @@ struct active_request {
   int32_t dropped = DPA_OK;  // DPA_ERROR_TIMEOUT / CANCELLED once dropped while running
 };
 
+// A returned request: one block holds all its arrays, in the server's pinned
+// response arena when it has room (the copies then run at the link's speed),
+// else in pageable heap memory.
 struct response_storage {
   dpa_response r{};
-  std::vector<float> positions, times, vertices, colors, ftle;
-  std::vector<uint64_t> remaining, indices64;
-  std::vector<uint32_t> indices32;
-  std::vector<uint8_t> termination;
+  char* data = nullptr;
+  uint64_t arena_offset = ~0ull;  // in units of kResponseUnit; ~0: heap
+  uint64_t arena_units = 0;
+  std::unique_ptr<char[]> heap;
 };
+
+constexpr uint64_t kResponseUnit = 256;
 
 }  // namespace
 
@@ -99,6 +104,8 @@ struct dpa_server {
       out_colors, out_indices;
   DeviceBuffer ftle_original, ftle_winners, ftle_flow, ftle_out;
   range_allocator slots, vertices;
+  PinnedBuffer response_arena;
+  range_allocator response_units;  // of response_arena, in kResponseUnit bytes
   std::vector<uint32_t> free_counters;
 
   std::mutex mutex;
@@ -411,31 +418,24 @@ uint32_t dpa_server::tick(uint64_t steps, int parity) {
 void dpa_server::finish(active_request& a, response_storage& out) {
   const dpa_request& q = a.p.request;
   const uint64_t n = q.count, first = a.first;
-  out.positions.resize(3 * n);
-  out.times.resize(n);
-  out.remaining.resize(n);
-  out.termination.resize(n);
-  if (n) {
-    SERVER_TRY(cudaMemcpyAsync(out.positions.data(), positions.as<float>() + 3 * first, n * 12,
-                               cudaMemcpyDeviceToHost, finish_stream));
-    SERVER_TRY(cudaMemcpyAsync(out.times.data(), times.as<float>() + first, n * 4,
-                               cudaMemcpyDeviceToHost, finish_stream));
-    SERVER_TRY(cudaMemcpyAsync(out.remaining.data(), remaining.as<uint64_t>() + first, n * 8,
-                               cudaMemcpyDeviceToHost, finish_stream));
-    SERVER_TRY(cudaMemcpyAsync(out.termination.data(), termination.as<uint8_t>() + first, n,
-                               cudaMemcpyDeviceToHost, finish_stream));
-  }
   // A request the worker dropped is returned as it stood, without curve or
   // FTLE -- unless every particle had finished before the drop took effect.
   int32_t status = DPA_OK;
-  if (a.dropped != DPA_OK) {
+  if (a.dropped != DPA_OK && n) {
+    std::vector<uint8_t> term(n);
+    SERVER_TRY(cudaMemcpyAsync(term.data(), termination.as<uint8_t>() + first, n,
+                               cudaMemcpyDeviceToHost, finish_stream));
     SERVER_TRY(cudaStreamSynchronize(finish_stream));
     for (uint64_t i = 0; i < n && status == DPA_OK; ++i)
-      if (out.termination[i] == DPA_TERMINATION_CANCELLED) status = a.dropped;
+      if (term[i] == DPA_TERMINATION_CANCELLED) status = a.dropped;
   }
+  const bool record = q.record && n && status == DPA_OK;
+  const bool ftle = q.ftle && n && status == DPA_OK;
   uint64_t vertex_count = 0, index_count = 0;
-  if (q.record && n && status == DPA_OK) {
-    // Emission of the request's curve, as one round of the reference.
+  const size_t index_bytes = q.index64 ? 8 : 4;
+  if (record) {
+    // Emission of the request's curve, as one round of the reference:
+    // offsets and totals first, to size the response.
     SERVER_TRY(raw_counts.reserve(n * 8));
     SERVER_TRY(vertex_offsets.reserve(n * 8));
     SERVER_TRY(segment_offsets.reserve(n * 8));
@@ -455,7 +455,62 @@ void dpa_server::finish(active_request& a, response_storage& out) {
     SERVER_TRY(cudaStreamSynchronize(finish_stream));
     vertex_count = totals[0];
     index_count = 2 * totals[1];
-    const size_t index_bytes = q.index64 ? 8 : 4;
+  }
+  dpa_response& r = out.r;
+  dpa::FtleArgs f{};
+  uint64_t cells = 0;
+  if (ftle) {
+    // Lattice FTLE of the final positions (ftle_estimator.cpp:7-65); the
+    // seeds should be the lattice of seed_stride on the request's field.
+    const dpa_field* field = fields[size_t(q.field)];
+    for (int i = 0; i < 3; ++i) {
+      const float stride = q.seed_stride[i] > 0.0f ? q.seed_stride[i] : 1.0f;
+      const float c = float(field->shape[i]) / stride;
+      f.shape[i] = c > 0.0f ? uint64_t(c) : 0;
+      f.offset[i] = field->offset[i];
+      f.spacing[i] = field->spacing[i] * stride;
+      f.two_spacing[i] = 2.0f * f.spacing[i];
+      r.ftle_shape[i] = f.shape[i];
+    }
+    cells = f.shape[0] * f.shape[1] * f.shape[2];
+  }
+  // One block for every array, each part 16-byte aligned.
+  auto pad = [](uint64_t b) { return (b + 15) / 16 * 16; };
+  const uint64_t part[8] = {pad(12 * n),           pad(4 * n),
+                            pad(8 * n),            pad(n),
+                            pad(12 * vertex_count), pad(4 * vertex_count),
+                            pad(index_bytes * index_count), pad(4 * cells)};
+  uint64_t at[8], bytes = 0;
+  for (int i = 0; i < 8; ++i) {
+    at[i] = bytes;
+    bytes += part[i];
+  }
+  {
+    std::lock_guard<std::mutex> lock(mutex);
+    const uint64_t units = (bytes + kResponseUnit - 1) / kResponseUnit;
+    uint64_t offset = 0;
+    if (bytes && response_units.allocate(units, &offset)) {
+      out.arena_offset = offset;
+      out.arena_units = units;
+      out.data = response_arena.as<char>() + offset * kResponseUnit;
+    }
+  }
+  if (!out.data) {
+    out.heap.reset(new char[std::max<uint64_t>(bytes, 16)]);  // not zero-filled
+    out.data = out.heap.get();
+  }
+  char* d = out.data;
+  if (n) {
+    SERVER_TRY(cudaMemcpyAsync(d + at[0], positions.as<float>() + 3 * first, n * 12,
+                               cudaMemcpyDeviceToHost, finish_stream));
+    SERVER_TRY(cudaMemcpyAsync(d + at[1], times.as<float>() + first, n * 4,
+                               cudaMemcpyDeviceToHost, finish_stream));
+    SERVER_TRY(cudaMemcpyAsync(d + at[2], remaining.as<uint64_t>() + first, n * 8,
+                               cudaMemcpyDeviceToHost, finish_stream));
+    SERVER_TRY(cudaMemcpyAsync(d + at[3], termination.as<uint8_t>() + first, n,
+                               cudaMemcpyDeviceToHost, finish_stream));
+  }
+  if (record) {
     SERVER_TRY(out_vertices.reserve(vertex_count * 12));
     SERVER_TRY(out_colors.reserve(vertex_count * 4));
     SERVER_TRY(out_indices.reserve(index_count * index_bytes));
@@ -472,78 +527,50 @@ void dpa_server::finish(active_request& a, response_storage& out) {
     e.colors = out_colors.as<float>();
     e.indices = out_indices.ptr;
     SERVER_TRY(dpa::launch_emit(e, q.index64 != 0, true, finish_stream));
-    out.vertices.resize(3 * vertex_count);
-    out.colors.resize(vertex_count);
-    SERVER_TRY(cudaMemcpyAsync(out.vertices.data(), out_vertices.ptr, vertex_count * 12,
+    SERVER_TRY(cudaMemcpyAsync(d + at[4], out_vertices.ptr, vertex_count * 12,
                                cudaMemcpyDeviceToHost, finish_stream));
-    SERVER_TRY(cudaMemcpyAsync(out.colors.data(), out_colors.ptr, vertex_count * 4,
+    SERVER_TRY(cudaMemcpyAsync(d + at[5], out_colors.ptr, vertex_count * 4,
                                cudaMemcpyDeviceToHost, finish_stream));
-    if (q.index64) {
-      out.indices64.resize(index_count);
-      SERVER_TRY(cudaMemcpyAsync(out.indices64.data(), out_indices.ptr, index_count * 8,
-                                 cudaMemcpyDeviceToHost, finish_stream));
-    } else {
-      out.indices32.resize(index_count);
-      SERVER_TRY(cudaMemcpyAsync(out.indices32.data(), out_indices.ptr, index_count * 4,
-                                 cudaMemcpyDeviceToHost, finish_stream));
-    }
+    SERVER_TRY(cudaMemcpyAsync(d + at[6], out_indices.ptr, index_count * index_bytes,
+                               cudaMemcpyDeviceToHost, finish_stream));
+  }
+  if (ftle && cells) {
+    SERVER_TRY(ftle_original.reserve(n * 12));
+    SERVER_TRY(ftle_winners.reserve(cells * 8));
+    SERVER_TRY(ftle_flow.reserve(cells * 12));
+    SERVER_TRY(ftle_out.reserve(cells * 4));
+    SERVER_TRY(cudaMemcpyAsync(ftle_original.ptr, a.p.positions.data(), n * 12,
+                               cudaMemcpyHostToDevice, finish_stream));
+    f.count = n;
+    f.original_positions = ftle_original.as<float>();
+    f.final_positions = positions.as<float>() + 3 * first;
+    f.mapping = DPA_FTLE_MAPPING_REFERENCE;
+    f.horizon = double(std::fabs(q.step_size * float(q.iterations)));
+    f.winners = ftle_winners.as<unsigned long long>();
+    f.flow = ftle_flow.as<float>();
+    f.ftle = ftle_out.as<float>();
+    SERVER_TRY(dpa::launch_ftle(f, finish_stream));
+    SERVER_TRY(cudaMemcpyAsync(d + at[7], ftle_out.ptr, cells * 4, cudaMemcpyDeviceToHost,
+                               finish_stream));
   }
   SERVER_TRY(cudaStreamSynchronize(finish_stream));
+  const uint64_t* rem_out = reinterpret_cast<const uint64_t*>(d + at[2]);
   uint64_t steps = 0;
-  for (uint64_t i = 0; i < n; ++i) steps += q.iterations - out.remaining[i];
-  dpa_response& r = out.r;
+  for (uint64_t i = 0; i < n; ++i) steps += q.iterations - rem_out[i];
   r.status = status;
-  if (q.ftle && n && status == DPA_OK) {
-    // Lattice FTLE of the final positions (ftle_estimator.cpp:7-65); the
-    // seeds should be the lattice of seed_stride on the request's field.
-    const dpa_field* field = fields[size_t(q.field)];
-    dpa::FtleArgs f{};
-    for (int i = 0; i < 3; ++i) {
-      const float stride = q.seed_stride[i] > 0.0f ? q.seed_stride[i] : 1.0f;
-      const float cells = float(field->shape[i]) / stride;
-      f.shape[i] = cells > 0.0f ? uint64_t(cells) : 0;
-      f.offset[i] = field->offset[i];
-      f.spacing[i] = field->spacing[i] * stride;
-      f.two_spacing[i] = 2.0f * f.spacing[i];
-      r.ftle_shape[i] = f.shape[i];
-    }
-    const uint64_t cells = f.shape[0] * f.shape[1] * f.shape[2];
-    if (cells) {
-      SERVER_TRY(ftle_original.reserve(n * 12));
-      SERVER_TRY(ftle_winners.reserve(cells * 8));
-      SERVER_TRY(ftle_flow.reserve(cells * 12));
-      SERVER_TRY(ftle_out.reserve(cells * 4));
-      SERVER_TRY(cudaMemcpyAsync(ftle_original.ptr, a.p.positions.data(), n * 12,
-                                 cudaMemcpyHostToDevice, finish_stream));
-      f.count = n;
-      f.original_positions = ftle_original.as<float>();
-      f.final_positions = positions.as<float>() + 3 * first;
-      f.mapping = DPA_FTLE_MAPPING_REFERENCE;
-      f.horizon = double(std::fabs(q.step_size * float(q.iterations)));
-      f.winners = ftle_winners.as<unsigned long long>();
-      f.flow = ftle_flow.as<float>();
-      f.ftle = ftle_out.as<float>();
-      SERVER_TRY(dpa::launch_ftle(f, finish_stream));
-      out.ftle.resize(cells);
-      SERVER_TRY(cudaMemcpyAsync(out.ftle.data(), ftle_out.ptr, cells * 4, cudaMemcpyDeviceToHost,
-                                 finish_stream));
-      SERVER_TRY(cudaStreamSynchronize(finish_stream));
-    }
-  }
   r.id = a.p.id;
   r.user = q.user;
   r.count = n;
-  r.positions = out.positions.data();
-  r.times = out.times.data();
-  r.remaining = out.remaining.data();
-  r.termination = out.termination.data();
+  r.positions = reinterpret_cast<const float*>(d + at[0]);
+  r.times = reinterpret_cast<const float*>(d + at[1]);
+  r.remaining = rem_out;
+  r.termination = reinterpret_cast<const uint8_t*>(d + at[3]);
   r.vertex_count = vertex_count;
-  r.vertices = out.vertices.empty() ? nullptr : out.vertices.data();
-  r.colors = out.colors.empty() ? nullptr : out.colors.data();
+  r.vertices = record ? reinterpret_cast<const float*>(d + at[4]) : nullptr;
+  r.colors = record ? reinterpret_cast<const float*>(d + at[5]) : nullptr;
   r.index_count = index_count;
-  r.indices = q.index64 ? static_cast<const void*>(out.indices64.data())
-                        : static_cast<const void*>(out.indices32.data());
-  r.ftle = out.ftle.empty() ? nullptr : out.ftle.data();
+  r.indices = record ? static_cast<const void*>(d + at[6]) : nullptr;
+  r.ftle = (ftle && cells) ? reinterpret_cast<const float*>(d + at[7]) : nullptr;
   r.particle_steps = steps;
   r.queued_seconds = a.p.queued;
   r.admitted_seconds = a.admitted;
@@ -723,6 +750,10 @@ int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_s
     if (e == cudaSuccess) e = s->raw.reserve(std::max<uint64_t>(v, 1) * 12);
     if (e == cudaSuccess) e = s->in_flight.reserve(4 * uint64_t(options->max_requests));
     if (e == cudaSuccess) e = s->work_counter.reserve(8);
+    const uint64_t response_bytes =
+        (options->response_bytes ? options->response_bytes : (256ull << 20)) / kResponseUnit *
+        kResponseUnit;
+    if (e == cudaSuccess) e = s->response_arena.reserve(response_bytes);
     if (e == cudaSuccess)
       e = cudaMemsetAsync(s->in_flight.ptr, 0, 4 * uint64_t(options->max_requests), s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
@@ -734,6 +765,7 @@ int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_s
     s->fields.reserve(kMaxServerFields);
     s->slots.reset(p);
     s->vertices.reset(v);
+    s->response_units.reset(response_bytes / kResponseUnit);
     s->admission.slot_capacity = p;
     s->admission.small_seeds = options->small_request_seeds ? options->small_request_seeds : 65536;
     s->admission.reserved_slots = p / 100 * std::min<uint32_t>(options->reserved_percent, 90);
@@ -839,7 +871,12 @@ int dpa_server_cancel(dpa_server* s, uint64_t id) {
 int dpa_server_release(dpa_server* s, uint64_t id) {
   if (!s) return DPA_ERROR_INVALID_ARGUMENT;
   std::lock_guard<std::mutex> lock(s->mutex);
-  return s->handed_out.erase(id) ? DPA_OK : DPA_ERROR_INVALID_ARGUMENT;
+  const auto it = s->handed_out.find(id);
+  if (it == s->handed_out.end()) return DPA_ERROR_INVALID_ARGUMENT;
+  if (it->second->arena_offset != ~0ull)
+    s->response_units.release(it->second->arena_offset, it->second->arena_units);
+  s->handed_out.erase(it);
+  return DPA_OK;
 }
 
 int dpa_server_get_stats(dpa_server* s, dpa_server_stats* out) {

@@ -38,12 +38,12 @@ class Server:
 
     def __init__(self, context, particle_capacity: int, vertex_capacity: int = 0,
                  steps_per_tick: int = 64, max_requests: int = 256, small_request_seeds: int = 0,
-                 reserved_percent: int = 0, max_bypass_ms: int = 0):
+                 reserved_percent: int = 0, max_bypass_ms: int = 0, response_bytes: int = 0):
         self.context = context
         self._lib = context._lib
         opts = N.ServerOptions(int(particle_capacity), int(vertex_capacity), int(steps_per_tick),
                                int(max_requests), int(small_request_seeds), int(reserved_percent),
-                               int(max_bypass_ms))
+                               int(max_bypass_ms), int(response_bytes))
         handle = C.c_void_p()
         context.check(self._lib.dpa_server_create(context.handle, C.byref(opts), C.byref(handle)))
         self.handle = handle
@@ -77,13 +77,23 @@ class Server:
         already returned."""
         return self._lib.dpa_server_cancel(self.handle, int(request_id)) == N.DPA_OK
 
-    def poll(self, wait_ms: int = 0) -> Result | None:
+    def poll(self, wait_ms: int = 0, copy_ids=None) -> Result | None:
+        """Takes one finished request. Its arrays are copied out unless
+        copy_ids is given and does not hold its id (then only its status,
+        counts and times come back)."""
         r = N.Response()
         got = C.c_int32()
         N.check(self._lib.dpa_server_poll(self.handle, int(wait_ms), C.byref(r), C.byref(got)),
                 self.context.handle)
         if not got.value:
             return None
+        if copy_ids is not None and int(r.id) not in copy_ids:
+            result = Result(int(r.id), int(r.status), None, None, None, None, None, None, None,
+                            int(r.particle_steps), r.queued_seconds, r.admitted_seconds,
+                            r.finished_seconds, None)
+            self._lib.dpa_server_release(self.handle, r.id)
+            self._index64.pop(r.id, None)
+            return result
         # A request dropped before admission returns no arrays.
         n = int(r.count) if r.positions else 0
         arr = lambda p, shape: np.ctypeslib.as_array(p, shape=shape).copy() if n else np.zeros(shape)

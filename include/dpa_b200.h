@@ -376,6 +376,9 @@ typedef struct dpa_server_options {
   uint32_t reserved_percent;   /* share of the slots kept for small requests (0-90) */
   uint32_t max_bypass_ms;      /* how long the oldest waiting request may be passed
                                   by younger ones that fit (0: 250 ms) */
+  uint64_t response_bytes;     /* pinned host memory for returned arrays (0: 256 MiB);
+                                  a response that does not fit it is returned from
+                                  pageable memory */
 } dpa_server_options;
 
 typedef struct dpa_request {
@@ -397,7 +400,9 @@ typedef struct dpa_request {
 } dpa_request;
 
 /* A finished request. Arrays are host memory owned by the server until
- * dpa_server_release(id). Times are seconds since the server started. */
+ * dpa_server_release(id) (pinned when the response arena has room; release
+ * promptly, a held response keeps its share of the arena). Times are seconds
+ * since the server started. */
 typedef struct dpa_response {
   uint64_t       id;
   void*          user;
@@ -462,7 +467,9 @@ int dpa_server_destroy(dpa_server* server);
  * Same inputs, outputs and results as dpa_advect_device (recording is not
  * offered); the ordering scratch comes from a fixed device array inside the
  * library (about 9 MiB, held by every GPU on which the library's code is
- * loaded until the process exits) instead of cudaMalloc. At most
+ * loaded until the process exits) instead of cudaMalloc. It checks its
+ * arguments as dpa_advect_device does and applies the context's tuning
+ * (dpa_context_set_tuning) the same way, so both give the same launches. At most
  * DPA_NO_ALLOC_MAX_PARTICLES particles per call; more is rejected with
  * DPA_ERROR_INVALID_ARGUMENT. The first call on a device resolves the array's
  * device address (and may load the library's code on that device), so make
