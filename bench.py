@@ -133,18 +133,30 @@ class ClockSampler:
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
 
-    def stop(self) -> dict:
+    def stop(self, window=None) -> dict:
+        """Median SM clock and the throttle reasons seen; with window = (t0,
+        t1) (perf_counter times of the timed region), only the samples taken
+        in it (or, when it is shorter than the sampling period, the three
+        nearest)."""
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        lines = self.lines
+        if window and lines:
+            t0, t1 = window
+            inside = [x for x in lines if t0 - 0.05 <= x[0] <= t1 + 0.05]
+            if len(inside) < 3:
+                mid = 0.5 * (t0 + t1)
+                inside = sorted(lines, key=lambda x: abs(x[0] - mid))[:3]
+            lines = inside
         sms, maxes, reasons = [], [], set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        for _, line in lines:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -1197,9 +1209,11 @@ def run_gpu(a):
     ctx.check(lib.dpa_context_launch_count(ctx.handle, C.byref(launches0)))
     clocks = ClockSampler(local)
     clocks.start()
+    time.sleep(0.5)  # nvidia-smi's first readings
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    t_begin = time.perf_counter()
     total_ms, kernel_ms, order_ms = 0.0, [], []
     for _ in range(a.steps):
         flush.fill_(2)
@@ -1217,7 +1231,9 @@ def run_gpu(a):
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    clock_info = clocks.stop()
+    t_end = time.perf_counter()
+    time.sleep(0.1)
+    clock_info = clocks.stop((t_begin, t_end))
     launches1 = C.c_uint64()
     ctx.check(lib.dpa_context_launch_count(ctx.handle, C.byref(launches1)))
     gpu_launches = int(launches1.value - launches0.value)

@@ -597,7 +597,7 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
     dpa_field* f = new dpa_field();
     f->owner = ctx;
     f->storage = storage;
-    const size_t node_bytes = storage == DPA_STORAGE_F32 ? 16 : 8;
+    const size_t node_bytes = dpa::field_node_bytes(storage);
     cudaError_t e = f->nodes.reserve(nodes * node_bytes);
     const float* src = xyzv;
     DeviceBuffer staging;
@@ -607,7 +607,8 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
         e = cudaMemcpyAsync(staging.ptr, xyzv, nodes * 12, cudaMemcpyHostToDevice, ctx->stream);
       src = staging.as<float>();
     }
-    if (e == cudaSuccess) e = dpa::launch_repack(src, nodes, storage, f->nodes.ptr, ctx->stream);
+    if (e == cudaSuccess)
+      e = dpa::launch_repack(src, nodes, uint32_t(shape[2]), storage, f->nodes.ptr, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     staging.release();
     if (e != cudaSuccess) {

@@ -169,8 +169,10 @@ cudaError_t launch_gather_probe(const float4* table, uint32_t mask, uint32_t sid
 cudaError_t launch_verify_division(float h, float y, float yl, unsigned int* mismatches,
                                    cudaStream_t stream);
 
-// Field repack: XYZV float [n][3] -> 4-wide nodes in the given storage.
-cudaError_t launch_repack(const float* xyzv, uint64_t nodes, int storage, void* out,
+// Field repack: XYZV float [n][3] (rows of n2 nodes along axis 2) -> the
+// device layout of the given storage; field_node_bytes is its size per node.
+uint64_t field_node_bytes(int storage);
+cudaError_t launch_repack(const float* xyzv, uint64_t nodes, uint32_t n2, int storage, void* out,
                           cudaStream_t stream);
 
 struct FtleArgs {
