@@ -324,8 +324,11 @@ def gather_peaks(ctx):
 
 def roofline(kernel_s, steps, particles, storage, key, peaks, samples_per_step=1):
     """The advection kernel's roofline: DRAM bytes against the measured HBM
-    copy bandwidth (the `bound` of the contract), and the resource that
-    saturates first (the L1TEX data path, against its measured ceiling)."""
+    copy bandwidth (the contract's `bound`; the bytes come from the committed
+    ncu capture of this workload, per particle-step, scaled by this run's
+    steps), and the resource that saturates first (`limiter`: the L1TEX data
+    path, from the same capture, with the load bandwidth of the gather
+    pattern measured in this run beside it)."""
     peak, peak_src = measured_peak_hbm()
     prof = traffic_profile(key)
     algorithmic = (BYTES_PER_STEP[storage] * samples_per_step * steps + STATE_BYTES * particles)
@@ -334,28 +337,32 @@ def roofline(kernel_s, steps, particles, storage, key, peaks, samples_per_step=1
            "algorithmic_gbs": algorithmic / kernel_s / 1e9,
            "algorithmic_bytes": f"{BYTES_PER_STEP[storage] * samples_per_step} B per particle-step "
                                 f"(8 corners x 3 components per field sample) + {STATE_BYTES} B "
-                                "per particle; the per-lane cell cache and L2 serve most of it, "
-                                "so it is not memory traffic"}
-    if prof:
-        traffic = prof["dram_bytes_per_step"] * steps
-        out.update({"achieved": traffic / kernel_s / 1e9, "traffic": traffic,
-                    "frac": traffic / kernel_s / 1e9 / peak,
-                    "traffic_source": f"{prof['capture']} ({prof['dram_bytes_per_step']:.2f} DRAM "
-                                      "B per particle-step, scaled by this run's steps)",
-                    "captured_with_current_sources": prof["captured_with_current_sources"]})
-        if peaks and prof.get("l1_bytes_per_step"):
-            l1 = prof["l1_bytes_per_step"] * steps / kernel_s / 1e9
-            out["limiter"] = {
-                "resource": "L1TEX data path (gather loads)", "achieved": l1,
-                "peak": peaks["l1_coalesced"], "frac": l1 / peaks["l1_coalesced"],
-                "unit": "GB/s",
-                "peak_source": "dpa_measure_gather_bandwidth, 64 KiB table, coalesced lanes",
-                "issue_active_pct": prof.get("issue_active_pct"),
-                "l1tex_throughput_pct": prof.get("l1tex_throughput_pct"),
-                "note": "L1TEX bytes per particle-step from the same capture"}
-    else:
+                                "per particle; the per-lane cell cache, L1 and L2 serve most of "
+                                "it, so it is not DRAM traffic"}
+    if peaks:
+        out["algorithmic_frac_of_l1_peak"] = out["algorithmic_gbs"] / peaks["l1_coalesced"]
+    if not prof:
         out.update({"achieved": None, "traffic": None, "frac": None,
                     "traffic_source": "no capture of this workload"})
+        return out
+    traffic = prof["dram_bytes_per_step"] * steps
+    out.update({"achieved": traffic / kernel_s / 1e9, "traffic": traffic,
+                "frac": traffic / kernel_s / 1e9 / peak,
+                "traffic_source": f"{prof['capture']}: {prof['dram_bytes_per_step']:.2f} DRAM B "
+                                  "per particle-step, scaled by this run's steps",
+                "captured_with_current_sources": prof["captured_with_current_sources"]})
+    if "l1tex_throughput_pct" in prof:
+        lim = {"resource": "L1TEX data path (the corner gathers' requests and sectors)",
+               "frac": prof["l1tex_throughput_pct"] / 100.0,
+               "frac_source": "ncu l1tex__throughput.avg.pct_of_peak_sustained_active",
+               "l1_sector_gbs": prof["l1_sector_bytes_per_step"] * steps / kernel_s / 1e9,
+               "issue_active_pct": prof["issue_active_pct"],
+               "warps_active_pct": prof["warps_active_pct"],
+               "long_scoreboard_stalls_per_issue": prof["long_scoreboard_per_issue"],
+               "warp_instructions_per_step": prof["warp_instructions_per_step"]}
+        if peaks:
+            lim["l1_gather_peaks_gbs"] = peaks
+        out["limiter"] = lim
     return out
 
 
