@@ -230,9 +230,9 @@ int dpa_field_create_unsteady(dpa_context* ctx, const float* xyzv, const uint64_
                               dpa_field** out);
 
 /* How the field's kernels divide a position by the spacing: 2 = power-of-two
- * spacings (one FMA of exact scaled values), 1 = Markstein's division by the
- * rounded reciprocal (one multiply and two FMAs), used only for spacings for
- * which it was checked on the device, at field creation, to give IEEE
+ * spacings (one FMA of exact scaled values), 1 = division by the reciprocal
+ * split into two floats (one multiply and one FMA), used only for spacings
+ * for which it was checked on the device, at field creation, to give IEEE
  * division's bits for every float dividend, 0 = IEEE division. All three give
  * the reference's rounded quotient. */
 int dpa_field_locate_mode(const dpa_field* field, int32_t* mode);
