@@ -82,7 +82,7 @@ int build_order(dpa_context* ctx, dpa_launch_scratch& scratch, const dpa_field* 
                 const float* positions, uint64_t count, cudaStream_t stream,
                 const uint32_t** order) {
   *order = nullptr;
-  if (count < 2) return DPA_OK;
+  if (count < dpa::kOrderMinParticles) return DPA_OK;
   DPA_TRY_CUDA(ctx, scratch.keys.reserve(count * 4));
   DPA_TRY_CUDA(ctx, scratch.values.reserve(count * 4));
   DPA_TRY_CUDA(ctx, scratch.sort_temp.reserve(dpa::kOrderCountsSize * 4));

@@ -97,7 +97,7 @@ extern "C" int dpa_advect_device_no_alloc(dpa_context* ctx, const dpa_field* fie
       if (e != cudaSuccess) return dpa::fail_cuda(ctx, e, "cudaEventRecord");
     }
     const uint32_t* order = nullptr;
-    if (options->morton_order && ctx->tuning.order && count >= 2) {
+    if (options->morton_order && ctx->tuning.order && count >= dpa::kOrderMinParticles) {
       // launch_order starts by zeroing the counters, so what an earlier call
       // left in the shared array does not matter.
       uint32_t* counts = reinterpret_cast<uint32_t*>(scratch + kCountsOffset);

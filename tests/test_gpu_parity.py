@@ -130,10 +130,11 @@ def test_half_storage_is_exact_on_the_rounded_field(ctx, oracle, storage):
 
 
 def test_morton_order_does_not_change_results(ctx, oracle):
+    # 12,000 particles: calls with fewer than 8192 run in input order anyway.
     grid = fields.curl_noise(32, 3.0, 2)
-    pos = _seeds_in_box(grid, 1500, 8)
-    a, _ = compare(ctx, oracle, grid, pos, 100, "euler", 0.3, 1500, True, morton=True)
-    b, _ = compare(ctx, oracle, grid, pos, 100, "euler", 0.3, 1500, True, morton=False)
+    pos = _seeds_in_box(grid, 12000, 8)
+    a, _ = compare(ctx, oracle, grid, pos, 100, "euler", 0.3, 12000, True, morton=True)
+    b, _ = compare(ctx, oracle, grid, pos, 100, "euler", 0.3, 12000, True, morton=False)
     np.testing.assert_array_equal(a.inactive_particles.position, b.inactive_particles.position)
 
 
@@ -315,11 +316,12 @@ def test_two_particles_per_lane_and_block_sizes_match_oracle(ctx, oracle, storag
     import ctypes as C
     import torch
     from dpa_b200 import _native as N
+    n = 10000  # enough to be sorted into the processing order
     grid = fields.curl_noise(48, 3.0, 15)
-    pos = _seeds_in_box(grid, 5000, 16)
+    pos = _seeds_in_box(grid, n, 16)
     data = grid.data if storage == "f32" else grid.data.astype(np.float16).astype(np.float32)
     og = oracle.OracleGrid(data, grid.spacing, grid.offset)
-    want = oracle.advect_round(og, integrator, 0.25, pos, np.full(5000, 300, np.uint64))
+    want = oracle.advect_round(og, integrator, 0.25, pos, np.full(n, 300, np.uint64))
     field = ctx.field(grid, storage)
     saved = N.Tuning()
     ctx.check(ctx._lib.dpa_context_get_tuning(ctx.handle, C.byref(saved)))
@@ -328,12 +330,12 @@ def test_two_particles_per_lane_and_block_sizes_match_oracle(ctx, oracle, storag
             t = N.Tuning(16, 0, 64, 0.0, block, ppt)
             ctx.check(ctx._lib.dpa_context_set_tuning(ctx.handle, C.byref(t)))
             p = torch.from_numpy(pos).cuda()
-            r = torch.full((5000,), 300, dtype=torch.int64, device="cuda")
-            term = torch.zeros(5000, dtype=torch.uint8, device="cuda")
+            r = torch.full((n,), 300, dtype=torch.int64, device="cuda")
+            term = torch.zeros(n, dtype=torch.uint8, device="cuda")
             opts = N.AdvectOptions(N.INTEGRATORS[integrator], 0.25, 0, 0, 0, 1, budget)
             for _ in range(300 // budget + 1 if budget else 1):
                 ctx.check(ctx._lib.dpa_advect_device(ctx.handle, field.handle, C.byref(opts),
-                                                     5000, C.c_void_p(p.data_ptr()),
+                                                     n, C.c_void_p(p.data_ptr()),
                                                      C.c_void_p(r.data_ptr()),
                                                      C.c_void_p(term.data_ptr()), None))
             ctx.synchronize()
