@@ -193,35 +193,10 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
     while (!__any_sync(kFull, halt)) {
       // An empty slot does not step: its NaN position would send IEEE
       // division into its slow path, which the whole warp would wait for.
-#if DPA_TAIL_PREFETCH
-      // The launch's end (the order is exhausted and the SM empties): issue
-      // slots are free, so each lane prefetches the cell its particle will
-      // reach if it keeps its last step's displacement.
-      if constexpr (!kUnsteady && kPPT == 1) {
-        if (exhausted && active[0]) {
-          const Position before = p[0];
-          r[0] = step<kIntegrator>(f, a.coefficients, sampler[0], p[0], t[0], history[0]);
-          if (r[0] == kStepTaken) {
-            Position ahead;
-            ahead.p0 = 2.0f * p[0].p0 - before.p0;
-            ahead.p21 = make_float2(2.0f * p[0].p21.x - before.p21.x,
-                                    2.0f * p[0].p21.y - before.p21.y);
-            prefetch_cell<kStorage>(f, ahead);
-          }
-        } else {
-          r[0] = active[0] ? step<kIntegrator>(f, a.coefficients, sampler[0], p[0], t[0],
-                                               history[0])
-                           : int(kStepOutOfBounds);
-        }
-      } else
-#endif
-      {
 #pragma unroll
-        for (int j = 0; j < kPPT; ++j)
-          r[j] = active[j] ? step<kIntegrator>(f, a.coefficients, sampler[j], p[j], t[j],
-                                               history[j])
-                           : int(kStepOutOfBounds);
-      }
+      for (int j = 0; j < kPPT; ++j)
+        r[j] = active[j] ? step<kIntegrator>(f, a.coefficients, sampler[j], p[j], t[j], history[j])
+                         : int(kStepOutOfBounds);
       halt = false;
 #pragma unroll
       for (int j = 0; j < kPPT; ++j) {

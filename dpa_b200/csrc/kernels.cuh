@@ -31,10 +31,6 @@ constexpr int kAdvectTrueRk4MinBlocks = DPA_ADVECT_TRUE_RK4_MIN_BLOCKS;
 #define DPA_ADVECT_PPT2_MIN_BLOCKS 2
 #endif
 constexpr int kAdvectPpt2MinBlocks = DPA_ADVECT_PPT2_MIN_BLOCKS;
-// At the launch's end, lanes prefetch the cell their particle heads for (1).
-#ifndef DPA_TAIL_PREFETCH
-#define DPA_TAIL_PREFETCH 0
-#endif
 // Launches whose particles would fill fewer blocks than the device has SMs
 // use smaller blocks (1) or keep kAdvectBlock threads per block (0).
 #ifndef DPA_ADVECT_SPREAD

@@ -146,32 +146,6 @@ __device__ __forceinline__ bool locate(const FieldView& f, const Position& p, ui
   return inside;
 }
 
-// Prefetches into L1 the four edges of the cell holding p (approximately
-// located: only a hint, whose address is in the field whenever the located
-// cell is inside it).
-template <int kStorage>
-__device__ __forceinline__ void prefetch_cell(const FieldView& f, const Position& p) {
-  const float q0 = (p.p0 - f.offset[0]) * f.reciprocal[0];
-  const float q1 = (p.p21.y - f.offset[1]) * f.reciprocal[1];
-  const float q2 = (p.p21.x - f.offset[2]) * f.reciprocal[2];
-  if (!(q0 >= 0.0f && q0 < f.upper[0] && q1 >= 0.0f && q1 < f.upper[1] && q2 >= 0.0f &&
-        q2 < f.upper[2]))
-    return;
-  const uint32_t node = __float2uint_rz(q0) * f.stride0 + __float2uint_rz(q1) * f.stride1 +
-                        __float2uint_rz(q2);
-#if DPA_EDGE_RECORDS
-  const uint64_t bytes = kStorage == DPA_STORAGE_F32 ? 32 : 16;
-#else
-  const uint64_t bytes = kStorage == DPA_STORAGE_F32 ? 16 : 8;
-#endif
-  const char* base = static_cast<const char*>(f.nodes) + uint64_t(node) * bytes;
-  const uint64_t s1 = uint64_t(f.stride1) * bytes, s0 = uint64_t(f.stride0) * bytes;
-  asm volatile("prefetch.global.L1 [%0];" ::"l"(base));
-  asm volatile("prefetch.global.L1 [%0];" ::"l"(base + s1));
-  asm volatile("prefetch.global.L1 [%0];" ::"l"(base + s0));
-  asm volatile("prefetch.global.L1 [%0];" ::"l"(base + s0 + s1));
-}
-
 // (1 - w) * lo + w * hi per lane, every operation rounded on its own.
 __device__ __forceinline__ float2 lerp2(float2 lo, float2 hi, float2 one_minus_w, float2 w) {
   return add2(mul2(one_minus_w, lo), mul2(w, hi));
