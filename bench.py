@@ -49,7 +49,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "RK4 particle-steps/s vs plain FP32 GPU & host TBB; served p50/p99 latency"
 UNIT = "particle-steps/s"
 FALLBACK_HBM_GBS = 6650.0
-BYTES_PER_STEP = {"f32": 96, "f16": 48, "bf16": 48}  # 8 corners x 3 components
+BYTES_PER_STEP = {"f32": 96, "f16": 48, "bf16": 48, "f32_edges": 96}  # 8 corners x 3 components
 STATE_BYTES = 12 + 8 + 12 + 8 + 1  # positions + remaining in, out + termination
 TRAFFIC_FILE = ROOT / "profiles" / "advect_traffic.json"
 
@@ -64,7 +64,7 @@ def parse_args():
                    choices=["throughput", "recording", "ftle", "batched", "serving"],
                    help="throughput: the headline line with every configuration; the others "
                         "print one configuration alone")
-    p.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16"])
+    p.add_argument("--storage", default="f32", choices=["f32", "f16", "bf16", "f32_edges"])
     p.add_argument("--integrator", default="runge_kutta_4")
     p.add_argument("--grid", dest="n", type=int, default=256,
                    help="grid points per axis of the throughput workload")
@@ -640,7 +640,10 @@ def ftle_config(ctx, stream, reps=10, warmup=3, checks=True):
     lattice = seeds.generate(offset, size, (grid.spacing * np.float32(2)).astype(np.float32),
                              250).position
     n, iterations, step = lattice.shape[0], 250, float(np.float32(0.02))
-    field = ctx.field(grid, "f32")
+    # F32 values as edge records (DPA_STORAGE_F32_EDGES): the same bits as F32
+    # node storage, one 32-byte load per cell edge for particles that change
+    # cells almost every step.
+    field = ctx.field(grid, "f32_edges")
     p0 = torch.from_numpy(lattice).cuda()
     r0 = torch.full((n,), iterations, dtype=torch.int64, device="cuda")
     p, r = torch.empty_like(p0), torch.empty_like(r0)
@@ -686,6 +689,11 @@ def ftle_config(ctx, stream, reps=10, warmup=3, checks=True):
         ftles.append(f)
     steps_taken = float(np.sum(iterations - r.cpu().numpy()))
     ms = statistics.mean(totals)
+    # The same lattice on F32 node storage, for comparison.
+    nodes = ctx.field(grid, "f32")
+    one(nodes.handle)
+    node_kernels = [one(nodes.handle)[1] for _ in range(3)]
+    nodes.close()
     # End to end: the host entry points with pinned arrays.
     hp, ht = _pinned((n, 3), np.float32), _pinned(n, np.uint8)
     hr = _pinned(n, np.int64).view(np.uint64)
@@ -709,15 +717,18 @@ def ftle_config(ctx, stream, reps=10, warmup=3, checks=True):
         "workload": "ABC + 5 % smoothed perturbation (sigma 3, seed 2) on 256^3 over "
                     "[0, 2 pi]^3, 128^3 seed lattice (stride 2), runge_kutta_4, step 0.02, "
                     "250 iterations, then FTLE (FP64 eigenvalue and log)",
+        "storage": "f32_edges (F32 values as one 32-byte record per cell edge; results "
+                   "identical to f32 node storage)",
         "value": steps_taken / (ms / 1e3), "unit": UNIT, "ms_per_step": ms,
         "particle_steps_per_step": steps_taken, "steps": reps, "warmup": warmup,
         "kernel_ms": statistics.mean(kernels), "ftle_ms": statistics.mean(ftles),
+        "kernel_ms_f32_node_storage": statistics.mean(node_kernels),
         "e2e": {"value": steps_taken / e2e, "unit": UNIT, "ms_per_step": e2e * 1e3,
                 "h2d_bytes_per_step": n * (12 + 8) + n * 24,
                 "d2h_bytes_per_step": n * (12 + 8 + 1) + 128 ** 3 * 4,
                 "call": "dpa_advect_round + dpa_ftle_estimate with pinned host arrays"},
         "roofline": roofline(statistics.mean(kernels) / 1e3, steps_taken, n, "f32",
-                             "ftle_lattice_f32", gather_peaks(ctx)),
+                             "ftle_lattice_f32_edges", gather_peaks(ctx)),
     }
     if not checks:
         field.close()

@@ -24,7 +24,7 @@ STATUS_NAMES = {
     8: "DPA_ERROR_CANCELLED",
 }
 
-STORAGE = {"f32": 0, "f16": 1, "bf16": 2}
+STORAGE = {"f32": 0, "f16": 1, "bf16": 2, "f32_edges": 3}
 
 INTEGRATORS = {
     "euler": 0,

@@ -26,8 +26,8 @@ LIBRARY = PACKAGE / "libdpa_b200.so"
 PIPELINE = PACKAGE / "bin" / "dpa_pipeline"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CUDA_SOURCES = ["capi.cu", "advect.cu", "advect_f32.cu", "advect_f16.cu", "advect_bf16.cu",
-                "emit.cu", "ftle.cu", "noalloc.cu", "serve.cu"]
+CUDA_SOURCES = ["capi.cu", "advect.cu", "advect_f32.cu", "advect_f32e.cu", "advect_f16.cu",
+                "advect_bf16.cu", "emit.cu", "ftle.cu", "noalloc.cu", "serve.cu"]
 
 
 def nvcc() -> str:

@@ -273,6 +273,11 @@ cudaError_t launch_advect(const FieldView& f, const AdvectArgs& a, int integrato
     case DPA_STORAGE_BF16:
       return unsteady ? launch_advect_storage<DPA_STORAGE_BF16, true>(f, a, integrator, record, stream)
                       : launch_advect_storage<DPA_STORAGE_BF16, false>(f, a, integrator, record, stream);
+    case DPA_STORAGE_F32_EDGES:
+      return unsteady
+                 ? launch_advect_storage<DPA_STORAGE_F32_EDGES, true>(f, a, integrator, record, stream)
+                 : launch_advect_storage<DPA_STORAGE_F32_EDGES, false>(f, a, integrator, record,
+                                                                        stream);
     default:
       return cudaErrorInvalidValue;
   }

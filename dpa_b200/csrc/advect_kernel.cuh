@@ -1,7 +1,8 @@
 // advect_kernel.cuh -- the advection kernel template and its launchers:
 // every step of a particle in registers (particle_advector.cpp:325-396), one
-// or two particles per lane. advect_f32.cu, advect_f16.cu and advect_bf16.cu
-// instantiate it per field storage, for steady and time-varying fields.
+// or two particles per lane. advect_f32.cu, advect_f32e.cu, advect_f16.cu and
+// advect_bf16.cu instantiate it per field storage, for steady and
+// time-varying fields.
 #pragma once
 
 #include <algorithm>

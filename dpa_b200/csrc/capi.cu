@@ -574,7 +574,8 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
   if (!ctx || !out || !shape || !offset || !spacing)
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "NULL argument");
   *out = nullptr;
-  if (storage != DPA_STORAGE_F32 && storage != DPA_STORAGE_F16 && storage != DPA_STORAGE_BF16)
+  if (storage != DPA_STORAGE_F32 && storage != DPA_STORAGE_F16 && storage != DPA_STORAGE_BF16 &&
+      storage != DPA_STORAGE_F32_EDGES)
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "unknown storage");
   for (int i = 0; i < 3; ++i) {
     if (shape[i] == 0 || shape[i] > (1u << 24))

@@ -260,47 +260,22 @@ __global__ void __launch_bounds__(kScanThreads) offsets_tiles_kernel(
   }
 }
 
-#if DPA_EDGE_RECORDS
-// Edge records (sample.cuh): record t holds nodes t and t + 1 along axis 2
-// (the last node of a row repeats itself; no cell reads that record's second
-// half).
+// Node layouts: one float4 (F32) or (x, y, z, 0) half/bfloat quad per node.
+// F32_EDGES: record t holds nodes t and t + 1 along axis 2, each component's
+// pair side by side (sample.cuh); the last node of a row repeats itself, and
+// no cell reads that record's second half.
 template <int kStorage>
 __global__ void repack_kernel(const float* xyzv, uint64_t nodes, uint32_t n2, void* out) {
   const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (t >= nodes) return;
-  const uint64_t u = (t % n2) + 1 < n2 ? t + 1 : t;
-  const float a[3] = {xyzv[3 * t], xyzv[3 * t + 1], xyzv[3 * t + 2]};
-  const float b[3] = {xyzv[3 * u], xyzv[3 * u + 1], xyzv[3 * u + 2]};
-  if constexpr (kStorage == DPA_STORAGE_F32) {
-    float4* o = reinterpret_cast<float4*>(out) + 2 * t;
-    o[0] = make_float4(a[0], b[0], a[1], b[1]);
-    o[1] = make_float4(a[2], b[2], 0.0f, 0.0f);
-  } else {
-    uint4 r;
-    unsigned w[4];
-    for (int c = 0; c < 3; ++c) {
-      if constexpr (kStorage == DPA_STORAGE_F16) {
-        const __half2 h = __floats2half2_rn(a[c], b[c]);
-        w[c] = *reinterpret_cast<const unsigned*>(&h);
-      } else {
-        const __nv_bfloat162 h = __floats2bfloat162_rn(a[c], b[c]);
-        w[c] = *reinterpret_cast<const unsigned*>(&h);
-      }
-    }
-    r.x = w[0];
-    r.y = w[1];
-    r.z = w[2];
-    r.w = 0u;
-    reinterpret_cast<uint4*>(out)[t] = r;
-  }
-}
-#else
-template <int kStorage>
-__global__ void repack_kernel(const float* xyzv, uint64_t nodes, uint32_t /*n2*/, void* out) {
-  const uint64_t t = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  if (t >= nodes) return;
   const float x = xyzv[3 * t], y = xyzv[3 * t + 1], z = xyzv[3 * t + 2];
-  if constexpr (kStorage == DPA_STORAGE_F32) {
+  if constexpr (kStorage == DPA_STORAGE_F32_EDGES) {
+    const uint64_t u = (t % n2) + 1 < n2 ? t + 1 : t;
+    float4* o = reinterpret_cast<float4*>(out) + 2 * t;
+    o[0] = make_float4(x, xyzv[3 * u], y, xyzv[3 * u + 1]);
+    o[1] = make_float4(z, xyzv[3 * u + 2], 0.0f, 0.0f);
+  } else if constexpr (kStorage == DPA_STORAGE_F32) {
+    (void)n2;
     reinterpret_cast<float4*>(out)[t] = make_float4(x, y, z, 0.0f);
   } else if constexpr (kStorage == DPA_STORAGE_F16) {
     const __half2 a = __floats2half2_rn(x, y);
@@ -318,7 +293,6 @@ __global__ void repack_kernel(const float* xyzv, uint64_t nodes, uint32_t /*n2*/
     reinterpret_cast<uint2*>(out)[t] = r;
   }
 }
-#endif
 
 inline unsigned blocks_for(uint64_t n, unsigned block) { return unsigned((n + block - 1) / block); }
 
@@ -368,11 +342,7 @@ cudaError_t launch_curve_offsets(const uint32_t* kept_vertices, const uint32_t* 
 }
 
 uint64_t field_node_bytes(int storage) {
-#if DPA_EDGE_RECORDS
-  return storage == DPA_STORAGE_F32 ? 32 : 16;
-#else
-  return storage == DPA_STORAGE_F32 ? 16 : 8;
-#endif
+  return storage == DPA_STORAGE_F32_EDGES ? 32 : storage == DPA_STORAGE_F32 ? 16 : 8;
 }
 
 cudaError_t launch_repack(const float* xyzv, uint64_t nodes, uint32_t n2, int storage, void* out,
@@ -388,6 +358,9 @@ cudaError_t launch_repack(const float* xyzv, uint64_t nodes, uint32_t n2, int st
       break;
     case DPA_STORAGE_BF16:
       repack_kernel<DPA_STORAGE_BF16><<<grid, 256, 0, stream>>>(xyzv, nodes, n2, out);
+      break;
+    case DPA_STORAGE_F32_EDGES:
+      repack_kernel<DPA_STORAGE_F32_EDGES><<<grid, 256, 0, stream>>>(xyzv, nodes, n2, out);
       break;
     default: return cudaErrorInvalidValue;
   }

@@ -95,7 +95,7 @@ cudaError_t launch_expand_ranges(const uint64_t* starts, const uint64_t* firsts,
 cudaError_t launch_advect(const FieldView& f, const AdvectArgs& a, int integrator, bool record,
                           cudaStream_t stream);
 // The instantiations of one storage for steady or time-varying fields
-// (advect_f32.cu, advect_f16.cu, advect_bf16.cu).
+// (advect_f32.cu, advect_f32e.cu, advect_f16.cu, advect_bf16.cu).
 template <int kStorage, bool kUnsteady>
 cudaError_t launch_advect_storage(const FieldView& f, const AdvectArgs& a, int integrator,
                                   bool record, cudaStream_t stream);

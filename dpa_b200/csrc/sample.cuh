@@ -15,10 +15,6 @@
 #ifndef DPA_F32_PACKED_LERP
 #define DPA_F32_PACKED_LERP 0
 #endif
-// Field layout: one record per node (0) or per cell edge along axis 2 (1).
-#ifndef DPA_EDGE_RECORDS
-#define DPA_EDGE_RECORDS 0
-#endif
 
 namespace dpa {
 
@@ -168,69 +164,22 @@ struct CornerNodes {
   float2 z04, z15, z26, z37;
 };
 
-// CornerEdges (F16 / BF16 nodes): z[e][c] = (component c of corner 2e,
-// component c of corner 2e + 1), the two ends of edge e = dx * 2 + dy along
-// axis 2, formed as the 16-bit values are widened. Each lerp is one packed
-// multiply of (lo, hi) by the weight pair (1 - w, w) and one scalar sum.
+// CornerEdges (F16 / BF16 nodes, F32 edge records): z[e][c] = (component c
+// of corner 2e, component c of corner 2e + 1), the two ends of edge
+// e = dx * 2 + dy along axis 2, formed as 16-bit values are widened or loaded
+// as they are from an edge record. Each lerp is one packed multiply of
+// (lo, hi) by the weight pair (1 - w, w) and one scalar sum. (F32 nodes in
+// this layout, pairs formed by register moves after the loads, measured 5 %
+// slower on the headline launch than CornerNodes.)
 struct CornerEdges {
   float2 z[4][3];
 };
 
-#if DPA_EDGE_RECORDS
-// Edge records: record n holds node n and node n + 1 along axis 2, each
-// component's two values side by side -- F32: (x_n, x_n+1, y_n, y_n+1, z_n,
-// z_n+1, 0, 0), 32 bytes, one 256-bit load; F16/BF16: the same eight 16-bit
-// values, 16 bytes, one 128-bit load. A cell's four edges are four loads
-// whose registers are already the (lo, hi) pairs the packed lerps take.
 template <int kStorage>
-using CornersOf = CornerEdges;
+using CornersOf = std::conditional_t<kStorage == DPA_STORAGE_F32, CornerNodes, CornerEdges>;
 
-template <int kStorage>
-constexpr int kRecordBytes = kStorage == DPA_STORAGE_F32 ? 32 : 16;
-
-template <int kStorage>
-__device__ __forceinline__ void load_edge(const char* record, float2 out[3]) {
-  if constexpr (kStorage == DPA_STORAGE_F32) {
-    float v[8];
-    asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]),
-          "=f"(v[7])
-        : "l"(record));
-    out[0] = make_float2(v[0], v[1]);
-    out[1] = make_float2(v[2], v[3]);
-    out[2] = make_float2(v[4], v[5]);
-  } else {
-    const uint4 r = __ldg(reinterpret_cast<const uint4*>(record));
-    const unsigned w[3] = {r.x, r.y, r.z};
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      if constexpr (kStorage == DPA_STORAGE_F16)
-        out[c] = __half22float2(*reinterpret_cast<const __half2*>(&w[c]));
-      else
-        out[c] = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w[c]));
-    }
-  }
-}
-
-template <int kStorage>
-__device__ __forceinline__ void gather(const FieldView& f, uint32_t node, CornerEdges& k,
-                                       int64_t slice_base = 0) {
-  const char* base = static_cast<const char*>(f.nodes) +
-                     (uint64_t(slice_base) + node) * uint64_t(kRecordBytes<kStorage>);
-  const uint64_t s1 = uint64_t(f.stride1) * kRecordBytes<kStorage>;
-  const uint64_t s0 = uint64_t(f.stride0) * kRecordBytes<kStorage>;
-  load_edge<kStorage>(base, k.z[0]);
-  load_edge<kStorage>(base + s1, k.z[1]);
-  load_edge<kStorage>(base + s0, k.z[2]);
-  load_edge<kStorage>(base + s0 + s1, k.z[3]);
-}
-#else
-template <int kStorage>
-using CornersOf =
-    std::conditional_t<kStorage == DPA_STORAGE_F32, CornerNodes, CornerEdges>;
-
-// The node type of a storage: one 16-byte float4 (F32) or 8-byte uint2 (F16,
-// BF16) per node.
+// Node layouts (F32, F16, BF16): one 16-byte float4 (F32) or 8-byte uint2
+// per node.
 template <int kStorage>
 using NodeOf = std::conditional_t<kStorage == DPA_STORAGE_F32, float4, uint2>;
 
@@ -248,6 +197,23 @@ struct CellEdges {
     e[3] = e[2] + f.stride1;
   }
 };
+
+// Edge records (F32_EDGES): record n holds node n and node n + 1 along axis
+// 2 with each component's two values side by side, (x_n, x_n+1, y_n, y_n+1,
+// z_n, z_n+1, 0, 0), 32 bytes read by one 256-bit load whose registers are
+// already the (lo, hi) pairs the packed lerps take.
+constexpr int kEdgeRecordBytes = 32;
+
+__device__ __forceinline__ void load_edge_record(const char* record, float2 out[3]) {
+  float v[8];
+  asm("ld.global.nc.v8.f32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+      : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]),
+        "=f"(v[7])
+      : "l"(record));
+  out[0] = make_float2(v[0], v[1]);
+  out[1] = make_float2(v[2], v[3]);
+  out[2] = make_float2(v[4], v[5]);
+}
 
 template <int kStorage>
 __device__ __forceinline__ void gather(const FieldView& f, uint32_t node, CornerNodes& k,
@@ -268,17 +234,27 @@ __device__ __forceinline__ void gather(const FieldView& f, uint32_t node, Corner
 template <int kStorage>
 __device__ __forceinline__ void gather(const FieldView& f, uint32_t node, CornerEdges& k,
                                        int64_t slice_base = 0) {
-  const CellEdges<kStorage> c(f, node, slice_base);
+  if constexpr (kStorage == DPA_STORAGE_F32_EDGES) {
+    const char* base = static_cast<const char*>(f.nodes) +
+                       (uint64_t(slice_base) + node) * uint64_t(kEdgeRecordBytes);
+    const uint64_t s1 = uint64_t(f.stride1) * kEdgeRecordBytes;
+    const uint64_t s0 = uint64_t(f.stride0) * kEdgeRecordBytes;
+    load_edge_record(base, k.z[0]);
+    load_edge_record(base + s1, k.z[1]);
+    load_edge_record(base + s0, k.z[2]);
+    load_edge_record(base + s0 + s1, k.z[3]);
+  } else {
+    const CellEdges<kStorage> c(f, node, slice_base);
 #pragma unroll
-  for (int e = 0; e < 4; ++e) {
-    float lo[3], hi[3];
-    load_node<kStorage>(c.e[e], 0, lo[0], lo[1], lo[2]);
-    load_node<kStorage>(c.e[e], 1, hi[0], hi[1], hi[2]);
+    for (int e = 0; e < 4; ++e) {
+      float lo[3], hi[3];
+      load_node<kStorage>(c.e[e], 0, lo[0], lo[1], lo[2]);
+      load_node<kStorage>(c.e[e], 1, hi[0], hi[1], hi[2]);
 #pragma unroll
-    for (int c2 = 0; c2 < 3; ++c2) k.z[e][c2] = make_float2(lo[c2], hi[c2]);
+      for (int c2 = 0; c2 < 3; ++c2) k.z[e][c2] = make_float2(lo[c2], hi[c2]);
+    }
   }
 }
-#endif
 
 __device__ __forceinline__ void trilinear(const CornerNodes& k, const Weights& w, float2& v01,
                                           float& v2) {

@@ -367,6 +367,7 @@ int run(const std::string& config_path) {
     int32_t storage = DPA_STORAGE_F32;
     if (args.storage == "f16") storage = DPA_STORAGE_F16;
     else if (args.storage == "bf16") storage = DPA_STORAGE_BF16;
+    else if (args.storage == "f32_edges") storage = DPA_STORAGE_F32_EDGES;
     else if (args.storage != "f32") throw std::runtime_error("unknown field storage " + args.storage);
     if (args.particle_advector_particles_per_round == 0)
       throw std::runtime_error("particle_advector_particles_per_round must be positive");

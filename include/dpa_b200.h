@@ -43,11 +43,16 @@ typedef enum dpa_status {
 } dpa_status;
 
 /* Device storage of a field. F32 keeps the reference's values exactly; F16 and
- * BF16 halve the gather bytes and interpolate in FP32. */
+ * BF16 halve the gather bytes and interpolate in FP32. F32_EDGES keeps the
+ * F32 values (results identical to F32) as one 32-byte record per cell edge
+ * along axis 2, twice F32's memory: a cell's corners are four loads instead
+ * of eight, which pays where particles change cells almost every step (dense
+ * FTLE lattices) and costs a little on sparse seeds in large fields. */
 typedef enum dpa_storage {
   DPA_STORAGE_F32 = 0,
   DPA_STORAGE_F16 = 1,
-  DPA_STORAGE_BF16 = 2
+  DPA_STORAGE_BF16 = 2,
+  DPA_STORAGE_F32_EDGES = 3
 } dpa_storage;
 
 /* Integrators. Codes 0-7 follow the alternatives of the reference's

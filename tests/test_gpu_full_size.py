@@ -88,7 +88,7 @@ def throughput_inputs():
     return grid, pos
 
 
-@pytest.mark.parametrize("storage", ["f32", "f16", "bf16"])
+@pytest.mark.parametrize("storage", ["f32", "f16", "bf16", "f32_edges"])
 def test_throughput_configuration_matches_the_oracle_on_a_sample(ctx, oracle, throughput_inputs,
                                                                  storage):
     grid, pos = throughput_inputs

@@ -129,6 +129,38 @@ def test_half_storage_is_exact_on_the_rounded_field(ctx, oracle, storage):
     compare(ctx, oracle, grid, pos, 300, "runge_kutta_4", 0.25, 2048, False, storage=storage)
 
 
+@pytest.mark.parametrize("case", ["abc_record", "noise_rk4", "spacing_0.7", "anisotropic",
+                                  "cash_karp"])
+def test_edge_record_storage_matches_the_f32_oracle(ctx, oracle, case):
+    # F32_EDGES holds the F32 values as one 32-byte record per cell edge:
+    # the same bits as F32 storage, so the oracle on the unrounded field.
+    if case == "abc_record":
+        grid = fields.abc(32)
+        pos = _seeds_in_box(grid, 1500, 3, box=([0, 0, 0], [2 * math.pi] * 3))
+        compare(ctx, oracle, grid, pos, 300, "runge_kutta_4", 0.01, 1000, True,
+                storage="f32_edges")
+    elif case == "noise_rk4":
+        grid = fields.curl_noise(64, 4.0, 11)
+        pos = _seeds_in_box(grid, 12000, 6)
+        compare(ctx, oracle, grid, pos, 300, "runge_kutta_4", 0.25, 12000, False,
+                storage="f32_edges")
+    elif case == "spacing_0.7":
+        grid = fields.curl_noise(48, 3.0, 9, spacing=0.7)
+        pos = _seeds_in_box(grid, 2048, 2)
+        compare(ctx, oracle, grid, pos, 200, "runge_kutta_4", 0.2, 2048, False,
+                storage="f32_edges")
+    elif case == "anisotropic":
+        data = fields.curl_noise(40, 3.0, 4).data[:, :17, :5].copy()
+        grid = dpa_b200.RegularGrid.from_data(data, (0.5, 2.0, 0.25), (1.0, -3.0, 0.5))
+        pos = _seeds_in_box(grid, 3000, 12)
+        compare(ctx, oracle, grid, pos, 150, "euler", 0.1, 3000, False, storage="f32_edges")
+    else:
+        grid = fields.curl_noise(32, 3.0, 5)
+        pos = _seeds_in_box(grid, 2000, 13)
+        compare(ctx, oracle, grid, pos, 200, "runge_kutta_cash_karp_54", 0.25, 2000, False,
+                storage="f32_edges")
+
+
 def test_morton_order_does_not_change_results(ctx, oracle):
     # 12,000 particles: calls with fewer than 8192 run in input order anyway.
     grid = fields.curl_noise(32, 3.0, 2)
@@ -228,10 +260,11 @@ def test_device_api_matches_host_api(ctx, oracle):
     np.testing.assert_array_equal(dt.cpu().numpy(), host.inactive_particles.termination)
 
 
-@pytest.mark.parametrize("mapping", ["reference", "lattice"])
-def test_ftle_matches_oracle(ctx, oracle, mapping):
+@pytest.mark.parametrize("mapping,storage", [("reference", "f32"), ("lattice", "f32"),
+                                             ("lattice", "f32_edges")])
+def test_ftle_matches_oracle(ctx, oracle, mapping, storage):
     grid = fields.abc_perturbed(64, seed=2)
-    field = ctx.field(grid)
+    field = ctx.field(grid, storage)
     offset, size = seeds.seed_box(grid)
     stride = np.float32(2)
     parts = seeds.generate(offset, size, (grid.spacing * stride).astype(np.float32), 60)
@@ -307,7 +340,7 @@ def test_reciprocal_division_matches_ieee_division_and_oracle(ctx, oracle, spaci
     assert modes == [1, 0], modes
 
 
-@pytest.mark.parametrize("storage", ["f32", "f16"])
+@pytest.mark.parametrize("storage", ["f32", "f16", "f32_edges"])
 @pytest.mark.parametrize("integrator", ["runge_kutta_4", "runge_kutta_cash_karp_54"])
 def test_two_particles_per_lane_and_block_sizes_match_oracle(ctx, oracle, storage, integrator):
     """Every launch shape the autotuner may pick -- 64 to 256 threads per
@@ -319,7 +352,7 @@ def test_two_particles_per_lane_and_block_sizes_match_oracle(ctx, oracle, storag
     n = 10000  # enough to be sorted into the processing order
     grid = fields.curl_noise(48, 3.0, 15)
     pos = _seeds_in_box(grid, n, 16)
-    data = grid.data if storage == "f32" else grid.data.astype(np.float16).astype(np.float32)
+    data = grid.data if storage != "f16" else grid.data.astype(np.float16).astype(np.float32)
     og = oracle.OracleGrid(data, grid.spacing, grid.offset)
     want = oracle.advect_round(og, integrator, 0.25, pos, np.full(n, 300, np.uint64))
     field = ctx.field(grid, storage)

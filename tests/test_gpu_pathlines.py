@@ -64,6 +64,19 @@ def test_half_storage_pathlines_match_the_rounded_field(ctx, oracle, gyre):
     _check(got, want)
 
 
+def test_edge_record_pathlines_match_the_oracle(ctx, oracle, gyre):
+    grid = gyre[0]
+    field = ctx.field(grid, "f32_edges")
+    try:
+        pos = _seeds(3000, 6)
+        want = oracle.advect_pathlines(grid, "runge_kutta_4", 0.05, pos, 0.5,
+                                       np.full(3000, 120, np.uint64))
+        got = advect_pathlines(ctx, field, pos, 0.5, 120, "runge_kutta_4", 0.05)
+        _check(got, want)
+    finally:
+        field.close()
+
+
 def test_step_budgets_resume_at_the_stored_time(ctx, oracle, gyre):
     grid, field, _ = gyre
     pos = _seeds(2000, 4)
