@@ -378,3 +378,78 @@ def test_two_particles_per_lane_and_block_sizes_match_oracle(ctx, oracle, storag
     finally:
         ctx.check(ctx._lib.dpa_context_set_tuning(ctx.handle, C.byref(saved)))
         field.close()
+
+
+def _signed_zero_field(n, spacing):
+    """v = (-z, -y, -x) stored reversed: every component is -0.0 on its own
+    face, so the sign of a zero weight decides the sign of a zero velocity
+    and, through x + dt * v, of a zero coordinate."""
+    data = np.zeros((n, n, n, 3), np.float32)
+    c = np.arange(n, dtype=np.float32) * np.float32(spacing)
+    data[..., 0] = -c[None, None, :]
+    data[..., 1] = -c[None, :, None]
+    data[..., 2] = -c[:, None, None]
+    return dpa_b200.RegularGrid.from_data(data, (spacing,) * 3)
+
+
+def _bits(a):
+    return np.ascontiguousarray(a, np.float32).view(np.uint32)
+
+
+@pytest.mark.parametrize("spacing", [1.0, 0.7])
+def test_signed_zeros_nan_field_values_and_huge_budgets(ctx, oracle, spacing):
+    """Bit for bit, signs of zero included: starts at -0.0 on each axis
+    (a zero weight keeps its sign as fmod's does), a NaN node in the field
+    (the velocity turns NaN, the next step leaves the grid), infinite starts,
+    and remaining counts above 2^32 that end out of bounds. Power-of-two and
+    general spacings; end positions through the device entry point and
+    recorded curves through rounds."""
+    import ctypes as C
+    import torch
+    from dpa_b200 import _native as N
+    grid = _signed_zero_field(8, spacing)
+    grid.data[5, 5, 5] = np.nan
+    h = np.float32(spacing)
+    mid = np.float32(1.5) * h
+    nan_cell = np.float32(4.5) * h
+    pos = np.array([[-0.0, mid, mid], [mid, -0.0, mid], [mid, mid, -0.0], [-0.0, -0.0, -0.0],
+                    [0.0, 0.0, 0.0], [nan_cell, nan_cell, nan_cell], [np.inf, mid, mid],
+                    [mid, -np.inf, mid], [mid, mid, mid], [np.float32(6.5) * h, mid, mid]],
+                   np.float32)
+    rem = np.array([3, 3, 3, 3, 3, 5, 4, 4, 2 ** 33, 2 ** 40 + 7], np.uint64)
+    og = oracle.OracleGrid.of(grid)
+    # Curves only for the first eight: a curve's staging spans the round's
+    # largest remaining count (particle_advector.cpp:311-316).
+    rec = slice(0, 8)
+    for integrator in ("euler", "runge_kutta_4"):
+        want = oracle.advect_round(og, integrator, 0.25, pos, rem)
+        assert np.isnan(want.positions[5]).all()  # the NaN node reached the particle
+        want_rec = oracle.advect_round(og, integrator, 0.25, pos[rec], rem[rec], record=True)
+        field = ctx.field(grid)
+        n = pos.shape[0]
+        p = torch.from_numpy(pos).cuda()
+        r = torch.from_numpy(rem.astype(np.int64)).cuda()
+        term = torch.zeros(n, dtype=torch.uint8, device="cuda")
+        opts = N.AdvectOptions(N.INTEGRATORS[integrator], 0.25, 0, 0, 0, 0, 0)
+        ctx.check(ctx._lib.dpa_advect_device(ctx.handle, field.handle, C.byref(opts), n,
+                                             C.c_void_p(p.data_ptr()), C.c_void_p(r.data_ptr()),
+                                             C.c_void_p(term.data_ptr()), None))
+        ctx.synchronize()
+        got = p.cpu().numpy()
+        finite = ~np.isnan(want.positions)
+        np.testing.assert_array_equal(np.isnan(got), ~finite)
+        np.testing.assert_array_equal(_bits(got)[finite], _bits(want.positions)[finite])
+        np.testing.assert_array_equal(r.cpu().numpy().astype(np.uint64), want.remaining)
+        np.testing.assert_array_equal(term.cpu().numpy(), want.termination)
+        adv = ParticleAdvector(ctx, n, "none", integrator, 0.25, False, True)
+        out = adv.advect(field, Particles(pos[rec].copy(), rem[rec].copy(), pos[rec].copy()))
+        field.close()
+        curve = out.integral_curves[0]
+        ok = ~np.isnan(want_rec.vertices)
+        np.testing.assert_array_equal(np.isnan(curve.vertices), ~ok)
+        np.testing.assert_array_equal(_bits(curve.vertices)[ok], _bits(want_rec.vertices)[ok])
+        np.testing.assert_array_equal(curve.indices, want_rec.indices)
+        np.testing.assert_array_equal(out.inactive_particles.termination, want_rec.termination)
+        done = out.inactive_particles
+        fin = ~np.isnan(want_rec.positions)
+        np.testing.assert_array_equal(_bits(done.position)[fin], _bits(want_rec.positions)[fin])
