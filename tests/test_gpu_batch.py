@@ -9,6 +9,7 @@ import pytest
 import dpa_b200
 from dpa_b200 import _native as N
 from dpa_b200 import fields, seeds
+from bitwise import assert_same
 
 pytestmark = pytest.mark.gpu
 
@@ -61,9 +62,9 @@ def test_step_budget_resumes_to_the_same_result(ctx, setup):
             break
         assert launches < 100
     assert launches >= 500 // 37
-    np.testing.assert_array_equal(pos.cpu().numpy(), want[0])
-    np.testing.assert_array_equal(rem.cpu().numpy(), want[1])
-    np.testing.assert_array_equal(term.cpu().numpy(), want[2])
+    assert_same(pos.cpu().numpy(), want[0])
+    assert_same(rem.cpu().numpy(), want[1])
+    assert_same(term.cpu().numpy(), want[2])
 
 
 def test_batched_sets_match_one_call(ctx, setup):
@@ -79,7 +80,7 @@ def test_batched_sets_match_one_call(ctx, setup):
         ctx.handle, field.handle, C.byref(opts), 5, offsets.ctypes.data_as(N._U64P), _ptr(pos),
         _ptr(rem), _ptr(term), steps.ctypes.data_as(N._U64P), None))
     ctx.synchronize()
-    np.testing.assert_array_equal(pos.cpu().numpy(), want[0])
+    assert_same(pos.cpu().numpy(), want[0])
     taken = r0.cpu().numpy() - want[1]
     for s in range(5):
         assert steps[s] == taken[offsets[s]:offsets[s + 1]].sum()
@@ -102,8 +103,8 @@ def test_graph_replay_matches_one_call(ctx, setup):
         torch.cuda.synchronize()
         ctx.check(ctx._lib.dpa_graph_launch(ctx.handle, graph, None))
         ctx.synchronize()
-        np.testing.assert_array_equal(pos.cpu().numpy(), want[0])
-        np.testing.assert_array_equal(term.cpu().numpy(), want[2])
+        assert_same(pos.cpu().numpy(), want[0])
+        assert_same(term.cpu().numpy(), want[2])
     ctx.check(ctx._lib.dpa_graph_destroy(ctx.handle, graph))
 
 
@@ -128,16 +129,16 @@ def test_graph_replays_after_a_larger_call_on_its_context(ctx, setup):
         torch.cuda.synchronize()
         ctx.check(ctx._lib.dpa_graph_launch(ctx.handle, graph, None))
         ctx.synchronize()
-        np.testing.assert_array_equal(pos.cpu().numpy(), want[0])
-        np.testing.assert_array_equal(rem.cpu().numpy(), want[1])
-        np.testing.assert_array_equal(term.cpu().numpy(), want[2])
+        assert_same(pos.cpu().numpy(), want[0])
+        assert_same(rem.cpu().numpy(), want[1])
+        assert_same(term.cpu().numpy(), want[2])
         big = reference_run(ctx, field, p0.repeat(4, 1), r0.repeat(4))
         if big_want is None:
             big_want = big
         for x, y in zip(big, big_want):
-            np.testing.assert_array_equal(x, y)
+            assert_same(x, y)
     for x, y in zip(big_want, want):
-        np.testing.assert_array_equal(x, np.concatenate([y] * 4))
+        assert_same(x, np.concatenate([y] * 4))
     ctx.check(ctx._lib.dpa_graph_destroy(ctx.handle, graph))
 
 
@@ -154,7 +155,7 @@ def test_autotune_keeps_results_identical(ctx, setup):
     assert best.measured_ms > 0
     got = reference_run(ctx, field, p0, r0)
     for g, w in zip(got, want):
-        np.testing.assert_array_equal(g, w)
+        assert_same(g, w)
     bad = N.Tuning(0, 0, 16, 0.0)
     with pytest.raises(dpa_b200.DpaError):
         ctx.check(ctx._lib.dpa_context_set_tuning(ctx.handle, C.byref(bad)))
@@ -191,9 +192,9 @@ def test_results_do_not_depend_on_launch_parameters(ctx, many, claim, blocks, or
         got = reference_run(ctx, field, pos, rem)
     finally:
         ctx.check(ctx._lib.dpa_context_set_tuning(ctx.handle, C.byref(saved)))
-    np.testing.assert_array_equal(got[0], want.positions)
-    np.testing.assert_array_equal(got[1].astype(np.uint64), want.remaining)
-    np.testing.assert_array_equal(got[2], want.termination)
+    assert_same(got[0], want.positions)
+    assert_same(got[1].astype(np.uint64), want.remaining)
+    assert_same(got[2], want.termination)
 
 
 def test_host_round_with_step_budget_reports_in_flight(ctx, setup):

@@ -25,6 +25,7 @@ import pytest
 import dpa_b200
 from dpa_b200 import ParticleAdvector, Particles, fields, seeds
 from dpa_b200 import _native as N
+from bitwise import assert_same
 
 pytestmark = pytest.mark.gpu
 
@@ -73,9 +74,9 @@ def _assert_sample_matches(oracle, data, grid, got, positions, remaining, sample
     og = oracle.OracleGrid(data, grid.spacing, grid.offset)
     want = oracle.advect_round(og, integrator, step, positions[sample],
                                np.asarray(remaining, np.uint64)[sample])
-    np.testing.assert_array_equal(got[2][sample], want.termination)
-    np.testing.assert_array_equal(got[1][sample], want.remaining)
-    np.testing.assert_array_equal(got[0][sample], want.positions)
+    assert_same(got[2][sample], want.termination)
+    assert_same(got[1][sample], want.remaining)
+    assert_same(got[0][sample], want.positions)
     return want
 
 
@@ -120,7 +121,7 @@ def test_throughput_configuration_does_not_depend_on_the_order(ctx, throughput_i
     finally:
         field.close()
     for x, y in zip(a, b):
-        np.testing.assert_array_equal(x, y)
+        assert_same(x, y)
 
 
 def test_recording_configuration_in_full(ctx, oracle):
@@ -139,11 +140,11 @@ def test_recording_configuration_in_full(ctx, oracle):
     og = oracle.OracleGrid.of(grid)
     want = oracle.advect_round(og, "runge_kutta_4", 0.01, parts.position,
                                np.full(4096, 1000, np.uint64), record=True)
-    np.testing.assert_array_equal(out.inactive_particles.termination, want.termination)
-    np.testing.assert_array_equal(out.inactive_particles.position, want.positions)
-    np.testing.assert_array_equal(curve.vertices, want.vertices)
+    assert_same(out.inactive_particles.termination, want.termination)
+    assert_same(out.inactive_particles.position, want.positions)
+    assert_same(curve.vertices, want.vertices)
     assert curve.indices.dtype == np.uint32  # 4096 * 1000 <= UINT32_MAX
-    np.testing.assert_array_equal(curve.indices, want.indices)
+    assert_same(curve.indices, want.indices)
     np.testing.assert_allclose(curve.colors, want.colors, rtol=0, atol=COLOR_ATOL)
     assert curve.vertices.shape[0] > 4096 * 100
 
@@ -163,13 +164,13 @@ def test_ftle_configuration_in_full(ctx, oracle):
     og = oracle.OracleGrid.of(grid)
     ref = oracle.advect_round(og, "runge_kutta_4", 0.02, parts.position,
                               np.full(len(parts), 250, np.uint64))
-    np.testing.assert_array_equal(out.termination, ref.termination)
-    np.testing.assert_array_equal(out.position, ref.positions)
+    assert_same(out.termination, ref.termination)
+    assert_same(out.position, ref.positions)
     want, _ = oracle.ftle(grid.shape, grid.offset, grid.spacing, (2, 2, 2), 250, 0.02,
                           out.original_position, ref.positions, 0)
     assert got.data.shape == want.shape == (128, 128, 128)
     finite = np.isfinite(want)
-    np.testing.assert_array_equal(np.isfinite(got.data), finite)
+    assert_same(np.isfinite(got.data), finite)
     np.testing.assert_allclose(got.data[finite], want[finite], rtol=FTLE_RTOL, atol=1e-6)
 
 
@@ -193,7 +194,7 @@ def test_batched_configuration_matches_single_calls_and_the_oracle(ctx, oracle):
     finally:
         field.close()
     for x, y in zip(batched, single):
-        np.testing.assert_array_equal(x, y)
+        assert_same(x, y)
     sample = np.sort(rng.choice(total, 2048, replace=False))
     _assert_sample_matches(oracle, _rounded(grid, "f16"), grid, batched, pos, rem, sample,
                            "runge_kutta_4", 0.25)

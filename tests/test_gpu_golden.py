@@ -9,6 +9,7 @@ import pytest
 import dpa_b200
 from dpa_b200 import ParticleAdvector, Particles
 from dpa_b200.advector import RegularGrid
+from bitwise import assert_same
 
 pytestmark = pytest.mark.gpu
 
@@ -35,14 +36,14 @@ def test_device_reproduces_the_fixture(ctx, path):
     finally:
         field.close()
     got = out.inactive_particles
-    np.testing.assert_array_equal(got.position, d["positions"])
-    np.testing.assert_array_equal(got.remaining_iterations, d["remaining"])
-    np.testing.assert_array_equal(got.termination, d["termination"])
+    assert_same(got.position, d["positions"])
+    assert_same(got.remaining_iterations, d["remaining"])
+    assert_same(got.termination, d["termination"])
     if record:
         curve = out.integral_curves[0]
-        np.testing.assert_array_equal(curve.vertices, d["vertices"])
+        assert_same(curve.vertices, d["vertices"])
         assert curve.indices.dtype == d["indices"].dtype
-        np.testing.assert_array_equal(curve.indices, d["indices"])
+        assert_same(curve.indices, d["indices"])
         np.testing.assert_allclose(curve.colors, d["colors"], rtol=0, atol=COLOR_ATOL)
 
 
@@ -53,11 +54,11 @@ def test_device_reproduces_the_ftle_fixture(ctx):
         adv = ParticleAdvector(ctx, len(d["seeds"]), "none", "runge_kutta_4", float(d["step"]),
                                False, False)
         out = adv.advect(field, Particles.create(d["seeds"], int(d["iterations"])))
-        np.testing.assert_array_equal(out.inactive_particles.position, d["positions"])
+        assert_same(out.inactive_particles.position, d["positions"])
         got = dpa_b200.estimate_ftle(ctx, field, int(d["iterations"]), d["stride"],
                                      float(d["step"]), out.inactive_particles)
     finally:
         field.close()
     finite = np.isfinite(d["ftle"])
-    np.testing.assert_array_equal(np.isfinite(got.data), finite)
+    assert_same(np.isfinite(got.data), finite)
     np.testing.assert_allclose(got.data[finite], d["ftle"][finite], rtol=FTLE_RTOL, atol=1e-6)

@@ -11,6 +11,7 @@ import pytest
 
 import dpa_b200
 from dpa_b200 import ParticleAdvector, Particles, fields, seeds
+from bitwise import assert_same
 
 pytestmark = pytest.mark.gpu
 
@@ -47,18 +48,18 @@ def compare(ctx, oracle, grid, positions, iterations, integrator, step, ppr, rec
         ctx.set_staging_limit(1 << 30)
     if host_chunk:
         ctx.check(ctx._lib.dpa_context_set_host_chunk_limit(ctx.handle, 256 << 20))
-    np.testing.assert_array_equal(got.inactive_particles.termination, want.termination)
-    np.testing.assert_array_equal(got.inactive_particles.remaining_iterations, want.remaining)
-    np.testing.assert_array_equal(got.inactive_particles.position, want.positions)
+    assert_same(got.inactive_particles.termination, want.termination)
+    assert_same(got.inactive_particles.remaining_iterations, want.remaining)
+    assert_same(got.inactive_particles.position, want.positions)
     if record:
         assert len(got.integral_curves) == len(want_rounds)
         for c, r in zip(got.integral_curves, want_rounds):
-            np.testing.assert_array_equal(c.vertices, r.vertices)
+            assert_same(c.vertices, r.vertices)
             assert c.indices.dtype == r.indices.dtype
-            np.testing.assert_array_equal(c.indices, r.indices)
+            assert_same(c.indices, r.indices)
             np.testing.assert_allclose(c.colors, r.colors, rtol=0, atol=COLOR_ATOL)
             special = (r.colors == 0) | (r.colors == np.float32(math.pi))
-            np.testing.assert_array_equal(c.colors[special], r.colors[special])
+            assert_same(c.colors[special], r.colors[special])
     return got, want
 
 
@@ -167,7 +168,7 @@ def test_morton_order_does_not_change_results(ctx, oracle):
     pos = _seeds_in_box(grid, 12000, 8)
     a, _ = compare(ctx, oracle, grid, pos, 100, "euler", 0.3, 12000, True, morton=True)
     b, _ = compare(ctx, oracle, grid, pos, 100, "euler", 0.3, 12000, True, morton=False)
-    np.testing.assert_array_equal(a.inactive_particles.position, b.inactive_particles.position)
+    assert_same(a.inactive_particles.position, b.inactive_particles.position)
 
 
 def test_edge_cases(ctx, oracle):
@@ -184,11 +185,11 @@ def test_edge_cases(ctx, oracle):
     og = oracle.OracleGrid.of(grid)
     want = oracle.advect_round(og, "runge_kutta_4", 0.01, pos, rem, record=True)
     got = adv.advect(field, Particles(pos.copy(), rem.copy(), pos.copy()))
-    np.testing.assert_array_equal(got.inactive_particles.termination, want.termination)
-    np.testing.assert_array_equal(got.inactive_particles.remaining_iterations, want.remaining)
+    assert_same(got.inactive_particles.termination, want.termination)
+    assert_same(got.inactive_particles.remaining_iterations, want.remaining)
     c = got.integral_curves[0]
-    np.testing.assert_array_equal(c.vertices, want.vertices)
-    np.testing.assert_array_equal(c.indices, want.indices)
+    assert_same(c.vertices, want.vertices)
+    assert_same(c.indices, want.indices)
     # zero field: zero-velocity termination at step 0
     zero = dpa_b200.RegularGrid.from_data(np.zeros((8, 8, 8, 3), np.float32), (1, 1, 1))
     zf = ctx.field(zero)
@@ -254,10 +255,10 @@ def test_device_api_matches_host_api(ctx, oracle):
                                          C.c_void_p(dp.data_ptr()), C.c_void_p(dr.data_ptr()),
                                          C.c_void_p(dt.data_ptr()), None))
     ctx.synchronize()
-    np.testing.assert_array_equal(dp.cpu().numpy(), host.inactive_particles.position)
-    np.testing.assert_array_equal(dr.cpu().numpy().astype(np.uint64),
+    assert_same(dp.cpu().numpy(), host.inactive_particles.position)
+    assert_same(dr.cpu().numpy().astype(np.uint64),
                                   host.inactive_particles.remaining_iterations)
-    np.testing.assert_array_equal(dt.cpu().numpy(), host.inactive_particles.termination)
+    assert_same(dt.cpu().numpy(), host.inactive_particles.termination)
 
 
 @pytest.mark.parametrize("mapping,storage", [("reference", "f32"), ("lattice", "f32"),
@@ -275,7 +276,7 @@ def test_ftle_matches_oracle(ctx, oracle, mapping, storage):
                              out.original_position, out.position, 0 if mapping == "reference" else 1)
     assert got.data.shape == want.shape == (32, 32, 32)
     finite = np.isfinite(want)
-    np.testing.assert_array_equal(np.isfinite(got.data), finite)
+    assert_same(np.isfinite(got.data), finite)
     np.testing.assert_allclose(got.data[finite], want[finite], rtol=1e-3, atol=1e-6)
 
 
@@ -329,10 +330,10 @@ def test_reciprocal_division_matches_ieee_division_and_oracle(ctx, oracle, spaci
             adv = ParticleAdvector(ctx, pos.shape[0], "none", "runge_kutta_4", step, False, True)
             got = adv.advect(field, Particles.create(pos, rem))
             field.close()
-            np.testing.assert_array_equal(got.inactive_particles.position, want.positions)
-            np.testing.assert_array_equal(got.inactive_particles.termination, want.termination)
-            np.testing.assert_array_equal(got.integral_curves[0].vertices, want.vertices)
-            np.testing.assert_array_equal(got.integral_curves[0].indices, want.indices)
+            assert_same(got.inactive_particles.position, want.positions)
+            assert_same(got.inactive_particles.termination, want.termination)
+            assert_same(got.integral_curves[0].vertices, want.vertices)
+            assert_same(got.integral_curves[0].indices, want.indices)
     finally:
         ctx.check(ctx._lib.dpa_context_set_ieee_division(ctx.handle, 0))
     # The split reciprocal is exact for these divisors (an exhaustive host
@@ -372,9 +373,9 @@ def test_two_particles_per_lane_and_block_sizes_match_oracle(ctx, oracle, storag
                                                      C.c_void_p(r.data_ptr()),
                                                      C.c_void_p(term.data_ptr()), None))
             ctx.synchronize()
-            np.testing.assert_array_equal(p.cpu().numpy(), want.positions)
-            np.testing.assert_array_equal(r.cpu().numpy().astype(np.uint64), want.remaining)
-            np.testing.assert_array_equal(term.cpu().numpy(), want.termination)
+            assert_same(p.cpu().numpy(), want.positions)
+            assert_same(r.cpu().numpy().astype(np.uint64), want.remaining)
+            assert_same(term.cpu().numpy(), want.termination)
     finally:
         ctx.check(ctx._lib.dpa_context_set_tuning(ctx.handle, C.byref(saved)))
         field.close()
@@ -437,19 +438,19 @@ def test_signed_zeros_nan_field_values_and_huge_budgets(ctx, oracle, spacing):
         ctx.synchronize()
         got = p.cpu().numpy()
         finite = ~np.isnan(want.positions)
-        np.testing.assert_array_equal(np.isnan(got), ~finite)
-        np.testing.assert_array_equal(_bits(got)[finite], _bits(want.positions)[finite])
-        np.testing.assert_array_equal(r.cpu().numpy().astype(np.uint64), want.remaining)
-        np.testing.assert_array_equal(term.cpu().numpy(), want.termination)
+        assert_same(np.isnan(got), ~finite)
+        assert_same(_bits(got)[finite], _bits(want.positions)[finite])
+        assert_same(r.cpu().numpy().astype(np.uint64), want.remaining)
+        assert_same(term.cpu().numpy(), want.termination)
         adv = ParticleAdvector(ctx, n, "none", integrator, 0.25, False, True)
         out = adv.advect(field, Particles(pos[rec].copy(), rem[rec].copy(), pos[rec].copy()))
         field.close()
         curve = out.integral_curves[0]
         ok = ~np.isnan(want_rec.vertices)
-        np.testing.assert_array_equal(np.isnan(curve.vertices), ~ok)
-        np.testing.assert_array_equal(_bits(curve.vertices)[ok], _bits(want_rec.vertices)[ok])
-        np.testing.assert_array_equal(curve.indices, want_rec.indices)
-        np.testing.assert_array_equal(out.inactive_particles.termination, want_rec.termination)
+        assert_same(np.isnan(curve.vertices), ~ok)
+        assert_same(_bits(curve.vertices)[ok], _bits(want_rec.vertices)[ok])
+        assert_same(curve.indices, want_rec.indices)
+        assert_same(out.inactive_particles.termination, want_rec.termination)
         done = out.inactive_particles
         fin = ~np.isnan(want_rec.positions)
-        np.testing.assert_array_equal(_bits(done.position)[fin], _bits(want_rec.positions)[fin])
+        assert_same(_bits(done.position)[fin], _bits(want_rec.positions)[fin])

@@ -9,6 +9,7 @@ import dpa_b200
 from dpa_b200 import _native as N
 from dpa_b200 import advect_pathlines, fields, seeds
 from dpa_b200.serve import Server
+from bitwise import assert_same
 
 pytestmark = pytest.mark.gpu
 
@@ -31,10 +32,10 @@ def _seeds(n, seed):
 
 
 def _check(got, want):
-    np.testing.assert_array_equal(got.termination, want.termination)
-    np.testing.assert_array_equal(got.remaining_iterations, want.remaining)
-    np.testing.assert_array_equal(got.position, want.positions)
-    np.testing.assert_array_equal(got.time, want.times)
+    assert_same(got.termination, want.termination)
+    assert_same(got.remaining_iterations, want.remaining)
+    assert_same(got.position, want.positions)
+    assert_same(got.time, want.times)
 
 
 @pytest.mark.parametrize("integrator", ["runge_kutta_4", "euler", "runge_kutta_4_true",
@@ -96,9 +97,9 @@ def test_step_budgets_resume_at_the_stored_time(ctx, oracle, gyre):
         ctx.synchronize()
         if not np.any(term.cpu().numpy() == 3):
             break
-    np.testing.assert_array_equal(p.cpu().numpy(), want.positions)
-    np.testing.assert_array_equal(t.cpu().numpy(), want.times)
-    np.testing.assert_array_equal(term.cpu().numpy(), want.termination)
+    assert_same(p.cpu().numpy(), want.positions)
+    assert_same(t.cpu().numpy(), want.times)
+    assert_same(term.cpu().numpy(), want.termination)
 
 
 def test_steady_calls_refuse_a_time_varying_field(ctx, gyre):
@@ -139,10 +140,10 @@ def test_served_pathlines_match_the_direct_call(ctx, gyre):
         res = results[rid]
         f = field if fid == g else steady
         want = advect_pathlines(ctx, f, pos, t0, iters, "runge_kutta_4", 0.05)
-        np.testing.assert_array_equal(res.positions, want.position)
-        np.testing.assert_array_equal(res.times, want.time)
-        np.testing.assert_array_equal(res.termination, want.termination)
+        assert_same(res.positions, want.position)
+        assert_same(res.times, want.time)
+        assert_same(res.termination, want.termination)
         if record:
             assert res.vertices.shape[0] > len(pos)
-            np.testing.assert_array_equal(res.vertices[0], pos[0])
+            assert_same(res.vertices[0], pos[0])
     steady.close()

@@ -11,6 +11,7 @@ import pytest
 import dpa_b200
 from dpa_b200 import ParticleAdvector, Particles, fields, seeds
 from dpa_b200.serve import Server
+from bitwise import assert_same
 
 pytestmark = pytest.mark.gpu
 
@@ -72,14 +73,14 @@ def test_results_are_the_same_alone_and_in_the_mix(ctx, resident):
         assert res.status == 0
         want = alone(ctx, resident[r["name"]][1], r["positions"], r["iterations"],
                      r["integrator"], r["step"], r["record"])
-        np.testing.assert_array_equal(res.positions, want.inactive_particles.position)
-        np.testing.assert_array_equal(res.termination, want.inactive_particles.termination)
-        np.testing.assert_array_equal(res.remaining, want.inactive_particles.remaining_iterations)
+        assert_same(res.positions, want.inactive_particles.position)
+        assert_same(res.termination, want.inactive_particles.termination)
+        assert_same(res.remaining, want.inactive_particles.remaining_iterations)
         if r["record"]:
             curve = want.integral_curves[0]
-            np.testing.assert_array_equal(res.vertices, curve.vertices)
-            np.testing.assert_array_equal(res.indices, curve.indices)
-            np.testing.assert_array_equal(res.colors, curve.colors)
+            assert_same(res.vertices, curve.vertices)
+            assert_same(res.indices, curve.indices)
+            assert_same(res.colors, curve.colors)
         assert res.queued <= res.admitted <= res.finished
 
 
@@ -96,7 +97,7 @@ def test_ftle_request_matches_the_stage_api(ctx, resident):
     assert res is not None and res.status == 0
     out = alone(ctx, field, lattice.position, 30, "runge_kutta_4", 0.02, False)
     want = dpa_b200.estimate_ftle(ctx, field, 30, (2, 2, 2), 0.02, out.inactive_particles)
-    np.testing.assert_array_equal(res.ftle, want.data)
+    assert_same(res.ftle, want.data)
 
 
 def test_admission_waits_for_room_and_refuses_what_never_fits(ctx, resident):
@@ -158,8 +159,8 @@ def test_many_concurrent_requests_all_complete(ctx, resident):
     for rid in ids:
         pos, iters, record = ids[rid]
         want = alone(ctx, field, pos, iters, "runge_kutta_4", 0.25, record)
-        np.testing.assert_array_equal(got[rid].positions, want.inactive_particles.position)
-        np.testing.assert_array_equal(got[rid].termination, want.inactive_particles.termination)
+        assert_same(got[rid].positions, want.inactive_particles.position)
+        assert_same(got[rid].termination, want.inactive_particles.termination)
         assert got[rid].particle_steps == int(
             (iters - want.inactive_particles.remaining_iterations.astype(np.int64)).sum())
 
@@ -180,8 +181,8 @@ def test_server_takes_memoryless_steppers_and_refuses_the_others(ctx, resident):
         res = server.poll(wait_ms=5000)
     assert res is not None and res.status == 0
     want = alone(ctx, field, pos, 80, "runge_kutta_cash_karp_54", 0.02, True)
-    np.testing.assert_array_equal(res.positions, want.inactive_particles.position)
-    np.testing.assert_array_equal(res.vertices, want.integral_curves[0].vertices)
+    assert_same(res.positions, want.inactive_particles.position)
+    assert_same(res.vertices, want.integral_curves[0].vertices)
 
 
 def test_deadlines_and_cancels_drop_requests_and_spare_the_rest(ctx, resident):
@@ -225,8 +226,8 @@ def test_deadlines_and_cancels_drop_requests_and_spare_the_rest(ctx, resident):
     for rid, s in zip(keep, small[1:]):
         assert results[rid].status == 0
         want = alone(ctx, field, s, 150, "runge_kutta_4", 0.25, False)
-        np.testing.assert_array_equal(results[rid].positions, want.inactive_particles.position)
-        np.testing.assert_array_equal(results[rid].termination,
+        assert_same(results[rid].positions, want.inactive_particles.position)
+        assert_same(results[rid].termination,
                                       want.inactive_particles.termination)
 
 
@@ -258,6 +259,6 @@ def test_small_requests_pass_a_large_one_that_waits_for_room(ctx, resident):
     assert all(results[s].admitted < results[second].admitted for s in smalls)
     for rid, s in zip(smalls, small):
         want = alone(ctx, field, s, 100, "runge_kutta_4", 0.25, False)
-        np.testing.assert_array_equal(results[rid].positions, want.inactive_particles.position)
+        assert_same(results[rid].positions, want.inactive_particles.position)
     want = alone(ctx, field, big, 300, "runge_kutta_4", 0.01, False)
-    np.testing.assert_array_equal(results[second].positions, want.inactive_particles.position)
+    assert_same(results[second].positions, want.inactive_particles.position)

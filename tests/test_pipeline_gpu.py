@@ -10,6 +10,7 @@ import pytest
 
 import dpa_b200
 from dpa_b200 import fields, host, seeds
+from bitwise import assert_same
 
 pytestmark = pytest.mark.gpu
 
@@ -57,10 +58,10 @@ def test_pipeline_curves_match_the_oracle(tmp_path, oracle):
     assert sorted(host.names(out)) == sorted(f"{k}_{i}" for i in range(3)
                                              for k in ("vertices", "colors", "indices"))
     for i, want in enumerate(rounds):
-        np.testing.assert_array_equal(host.read(out, f"vertices_{i}").reshape(-1, 3), want.vertices)
+        assert_same(host.read(out, f"vertices_{i}").reshape(-1, 3), want.vertices)
         idx = host.read(out, f"indices_{i}")
         assert host.info(out, f"indices_{i}")[2] == 4  # uint32 (pipeline.cpp:155)
-        np.testing.assert_array_equal(idx, want.indices.astype(np.uint64))
+        assert_same(idx, want.indices.astype(np.uint64))
         np.testing.assert_allclose(host.read(out, f"colors_{i}"), want.colors, rtol=0, atol=2e-6)
 
     xdmf = (tmp_path / "result.rank_0.h5.xdmf").read_text()
@@ -102,7 +103,7 @@ def test_pipeline_ftle_matches_the_oracle(tmp_path, oracle):
     got = host.read(path, "data")
     assert got.shape == want.shape == (24, 24, 24)
     finite = np.isfinite(want)
-    np.testing.assert_array_equal(np.isfinite(got), finite)
+    assert_same(np.isfinite(got), finite)
     np.testing.assert_allclose(got[finite], want[finite], rtol=1e-3, atol=1e-6)
     xdmf = (tmp_path / "result.rank_0_grid.h5.xdmf").read_text()
     assert "3DCoRectMesh" in xdmf and 'NumberOfElements="24 24 24"' in xdmf
@@ -122,7 +123,7 @@ def test_device_seed_generators_match_the_host(ctx):
                                          C.byref(n), C.c_void_p(out.data_ptr()), None))
     ctx.synchronize()
     assert n.value == 5000
-    np.testing.assert_array_equal(out.cpu().numpy(), host.random_seeds(offset, size, 5000, 11))
+    assert_same(out.cpu().numpy(), host.random_seeds(offset, size, 5000, 11))
     stride = np.float32([0.5, 0.25, 0.75])
     shape = (C.c_uint64 * 3)()
     ctx.check(lib.dpa_seed_lattice_device(ctx.handle, f3(offset), f3(size), f3(stride), None,
@@ -131,4 +132,4 @@ def test_device_seed_generators_match_the_host(ctx):
     ctx.check(lib.dpa_seed_lattice_device(ctx.handle, f3(offset), f3(size), f3(stride), None,
                                           C.byref(n), shape, C.c_void_p(lat.data_ptr()), None))
     ctx.synchronize()
-    np.testing.assert_array_equal(lat.cpu().numpy(), host.lattice_seeds(offset, size, stride))
+    assert_same(lat.cpu().numpy(), host.lattice_seeds(offset, size, stride))

@@ -13,6 +13,7 @@ import ctypes as C
 
 import numpy as np
 import pytest
+from bitwise import assert_same
 
 pytestmark = pytest.mark.gpu
 
@@ -62,7 +63,7 @@ def test_no_alloc_matches_the_allocating_entry_point():
         for i in range(len(counts)):
             got = run(lib.dpa_advect_device_no_alloc, i)
             for g, w in zip(got, want[i]):
-                np.testing.assert_array_equal(g, w)
+                assert_same(g, w)
         if call == 0:
             free_before = torch.cuda.mem_get_info()[0]
     assert torch.cuda.mem_get_info()[0] == free_before
@@ -127,14 +128,14 @@ def test_no_alloc_small_counts_orders_and_resumption(morton_order, tuned):
             want_state = call(lib.dpa_advect_device, p0, 200, budget)
             got_state = call(lib.dpa_advect_device_no_alloc, p0, 200, budget)
             for g, w in zip(host(got_state), host(want_state)):
-                np.testing.assert_array_equal(g, w)
+                assert_same(g, w)
             if budget:
                 # Resume both from their in-flight states, twice.
                 for _ in range(2):
                     want_state = call(lib.dpa_advect_device, p0, 200, budget, want_state)
                     got_state = call(lib.dpa_advect_device_no_alloc, p0, 200, budget, got_state)
                     for g, w in zip(host(got_state), host(want_state)):
-                        np.testing.assert_array_equal(g, w)
+                        assert_same(g, w)
 
     # The same argument checks as dpa_advect_device: a non-finite step size.
     bad = N.AdvectOptions(N.INTEGRATORS["runge_kutta_4"], float("nan"), 0, 0, 0, 1, 0)
