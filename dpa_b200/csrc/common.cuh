@@ -86,6 +86,25 @@ __device__ __forceinline__ float divide_spacing(float a, float h, float y, float
   else return divide_by_reciprocal(a, h, y, yl);
 }
 
+// Three divisions by known divisors (a_i / h_i, reciprocal pairs y_i, yl_i):
+// one range test for all three dividends instead of one each. Inside the
+// range every quotient is the reciprocal form's, as divide_by_reciprocal
+// gives; otherwise each takes divide_by_reciprocal's own test. (fminf and
+// fmaxf pass over NaN, but a NaN dividend gives NaN on either path.)
+__device__ __forceinline__ void divide3_by_reciprocal(const float a[3], const float h[3],
+                                                      const float y[3], const float yl[3],
+                                                      float q[3]) {
+  const float lo = fminf(fminf(fabsf(a[0]), fabsf(a[1])), fabsf(a[2]));
+  const float hi = fmaxf(fmaxf(fabsf(a[0]), fabsf(a[1])), fabsf(a[2]));
+  if (lo >= 0x1p-64f && hi <= 0x1p64f) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) q[i] = __fmaf_rn(a[i], y[i], __fmul_rn(a[i], yl[i]));
+  } else {
+#pragma unroll
+    for (int i = 0; i < 3; ++i) q[i] = divide_by_reciprocal(a[i], h[i], y[i], yl[i]);
+  }
+}
+
 // Integrator id of the kernel instantiation shared by the reference's other
 // odeint steppers (modified_midpoint, runge_kutta_cash_karp54,
 // runge_kutta_dopri5, runge_kutta_fehlberg78, adams_bashforth<2>,

@@ -76,6 +76,14 @@ struct Weights {
   float2 w21;
 };
 
+// fmod(a, h) from the floor s of the rounded quotient a / h.
+__device__ __forceinline__ float remainder_general(float a, float s, float h) {
+  float r = fmaf(-s, h, a);
+  if (r < 0.0f) r = __fadd_rn(r, h);
+  if (r == 0.0f) r = copysignf(0.0f, a);
+  return r;
+}
+
 // Where a position falls in the grid, per axis: the rounded quotient
 // q = (p - offset) / h, its floor s (the cell subscript) and the weight
 // w = fmod(p - offset, h) / h, all as the reference rounds them. The position
@@ -94,10 +102,7 @@ struct Weights {
 // reciprocal pair (kLocateReciprocal), which gives the same bits.
 template <int kLocate>
 __device__ __forceinline__ float weight_general(float a, float s, float h, float y, float yl) {
-  float r = fmaf(-s, h, a);
-  if (r < 0.0f) r = __fadd_rn(r, h);
-  if (r == 0.0f) r = copysignf(0.0f, a);
-  return divide_spacing<kLocate>(r, h, y, yl);
+  return divide_spacing<kLocate>(remainder_general(a, s, h), h, y, yl);
 }
 
 // Locates p; node receives the index of the cell's first corner within its
@@ -120,9 +125,18 @@ __device__ __forceinline__ bool locate(const FieldView& f, const Position& p, ui
   } else {
     a0 = __fsub_rn(p.p0, f.offset[0]);
     a21 = sum2(p.p21, neg2(make_float2(f.offset[2], f.offset[1])));
-    q0 = divide_spacing<kLocate>(a0, f.spacing[0], f.reciprocal[0], f.reciprocal_lo[0]);
-    q2 = divide_spacing<kLocate>(a21.x, f.spacing[2], f.reciprocal[2], f.reciprocal_lo[2]);
-    q1 = divide_spacing<kLocate>(a21.y, f.spacing[1], f.reciprocal[1], f.reciprocal_lo[1]);
+    if constexpr (kLocate == kLocateReciprocal) {
+      const float a[3] = {a0, a21.y, a21.x};
+      float q[3];
+      divide3_by_reciprocal(a, f.spacing, f.reciprocal, f.reciprocal_lo, q);
+      q0 = q[0];
+      q1 = q[1];
+      q2 = q[2];
+    } else {
+      q0 = divide_spacing<kLocate>(a0, f.spacing[0], f.reciprocal[0], f.reciprocal_lo[0]);
+      q2 = divide_spacing<kLocate>(a21.x, f.spacing[2], f.reciprocal[2], f.reciprocal_lo[2]);
+      q1 = divide_spacing<kLocate>(a21.y, f.spacing[1], f.reciprocal[1], f.reciprocal_lo[1]);
+    }
   }
   const bool inside = (q0 >= 0.0f) && (q0 < f.upper[0]) && (q1 >= 0.0f) && (q1 < f.upper[1]) &&
                       (q2 >= 0.0f) && (q2 < f.upper[2]);
@@ -131,6 +145,15 @@ __device__ __forceinline__ bool locate(const FieldView& f, const Position& p, ui
     w.w0 = copysignf(__fsub_rn(q0, s0), q0);
     const float2 d = sum2(make_float2(q2, q1), neg2(make_float2(s2, s1)));
     w.w21 = make_float2(copysignf(d.x, q2), copysignf(d.y, q1));
+  } else if constexpr (kLocate == kLocateReciprocal) {
+    const float a[3] = {a0, a21.y, a21.x};
+    const float s[3] = {s0, s1, s2};
+    float r[3], ww[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) r[i] = remainder_general(a[i], s[i], f.spacing[i]);
+    divide3_by_reciprocal(r, f.spacing, f.reciprocal, f.reciprocal_lo, ww);
+    w.w0 = ww[0];
+    w.w21 = make_float2(ww[2], ww[1]);
   } else {
     w.w0 = weight_general<kLocate>(a0, s0, f.spacing[0], f.reciprocal[0], f.reciprocal_lo[0]);
     w.w21 = make_float2(
