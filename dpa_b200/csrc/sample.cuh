@@ -354,6 +354,24 @@ struct CellSampler {
     return true;
   }
 
+  // sample() without the early return, for a caller that selects its result:
+  // an outside position loads no corners, and its sample (from the cached
+  // ones) is to be discarded.
+  __device__ __forceinline__ bool sample_selected(const FieldView& f, const Position& p,
+                                                  float2& v01, float& v2) {
+    uint32_t node;
+    Weights w;
+    const bool inside = locate<kLocate>(f, p, node, w);
+    if (inside && node != cached) {
+      gather<kStorage>(f, node, corners);
+      cached = node;
+    }
+    trilinear(corners, w, v01, v2);
+    return inside;
+  }
+
+  static constexpr bool kSteady = true;
+
   __device__ __forceinline__ void reset() { cached = ~0u; }
 };
 
@@ -412,6 +430,8 @@ struct TimeSampler {
     v2 = __fadd_rn(__fmul_rn(u, a2), __fmul_rn(wt, b2));
     return true;
   }
+
+  static constexpr bool kSteady = false;
 
   __device__ __forceinline__ void reset() {
     cached = ~0u;
@@ -503,6 +523,29 @@ __device__ __forceinline__ int step(const FieldView& f, const StepCoefficients& 
                                    StepHistory& history) {
   float2 v01;
   float v2;
+  if constexpr (Sampler::kSteady && (kIntegrator == DPA_INTEGRATOR_EULER ||
+                                     kIntegrator == DPA_INTEGRATOR_RUNGE_KUTTA_4)) {
+    // Without branches on the outcome: the step is computed whatever the
+    // sample, and kept only when the position was inside and the velocity
+    // not zero (a step's latency is a dependent chain; the launch's end and
+    // launches of few particles wait for it).
+    const bool inside = sampler.sample_selected(f, p, v01, v2);
+    const bool zero = is_zero(v01, v2);
+    Position n = p;
+    if constexpr (kIntegrator == DPA_INTEGRATOR_EULER) {
+      n.p0 = __fadd_rn(p.p0, __fmul_rn(k.dt, v2));
+      n.p21 = add2(p.p21, mul2(splat(k.dt), v01));
+    } else {
+      const float m0 = __fmul_rn(k.c0, v2), m1 = __fmul_rn(k.c1, v2);
+      n.p0 = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(p.p0, m0), m1), m1), m0);
+      const float2 n0 = mul2(splat(k.c0), v01), n1 = mul2(splat(k.c1), v01);
+      n.p21 = add2(add2(add2(add2(p.p21, n0), n1), n1), n0);
+    }
+    const bool taken = inside && !zero;
+    p.p0 = taken ? n.p0 : p.p0;
+    p.p21 = make_float2(taken ? n.p21.x : p.p21.x, taken ? n.p21.y : p.p21.y);
+    return !inside ? int(kStepOutOfBounds) : zero ? int(kStepZeroVelocity) : int(kStepTaken);
+  }
   if (!sampler.sample(f, p, t, v01, v2)) return kStepOutOfBounds;
   if (is_zero(v01, v2)) return kStepZeroVelocity;
   if constexpr (kIntegrator == DPA_INTEGRATOR_EULER) {
