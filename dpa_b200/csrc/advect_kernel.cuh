@@ -25,11 +25,11 @@ struct CurveCounter {
   bool prev_open = false;  // previous kept vertex is not terminal-valued
 
   __device__ __forceinline__ void append(float x, float y, float z) {
-    if (equals3(x, y, z, kInvalid)) return;
+    const bool valid = !equals3(x, y, z, kInvalid);
     const bool terminal = equals3(x, y, z, kTerminal);
-    if (!terminal && prev_open) ++segments;
-    prev_open = !terminal;
-    ++kept;
+    segments += valid && !terminal && prev_open ? 1u : 0u;
+    prev_open = valid ? !terminal : prev_open;
+    kept += valid ? 1u : 0u;
   }
 };
 
@@ -201,20 +201,19 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
       halt = false;
 #pragma unroll
       for (int j = 0; j < kPPT; ++j) {
-        if (r[j] == kStepTaken) {  // never for an empty slot
-          ++it[j];
-          if constexpr (kUnsteady) t[j] = __fadd_rn(t[j], a.coefficients.dt);
-          if constexpr (kRecord) {
+        const bool taken = r[j] == kStepTaken;  // never for an empty slot
+        it[j] += taken ? 1u : 0u;
+        if constexpr (kUnsteady) t[j] = taken ? __fadd_rn(t[j], a.coefficients.dt) : t[j];
+        if constexpr (kRecord) {
+          if (taken) {
             float* v = curve[j] + 3 * uint64_t(it[j]);
             v[0] = p[j].p0;
             v[1] = p[j].p21.y;
             v[2] = p[j].p21.x;
             counter[j].append(p[j].p0, p[j].p21.y, p[j].p21.x);
           }
-          stop[j] = it[j] >= limit[j];
-        } else {
-          stop[j] = true;
         }
+        stop[j] = !taken || it[j] >= limit[j];
         halt = halt || (active[j] && stop[j]);
       }
     }

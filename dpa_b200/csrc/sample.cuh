@@ -160,8 +160,10 @@ __device__ __forceinline__ bool locate(const FieldView& f, const Position& p, ui
         weight_general<kLocate>(a21.x, s2, f.spacing[2], f.reciprocal[2], f.reciprocal_lo[2]),
         weight_general<kLocate>(a21.y, s1, f.spacing[1], f.reciprocal[1], f.reciprocal_lo[1]));
   }
-  // Saturating conversions: outside the grid the value is never used.
-  node = __float2uint_rz(s0) * f.stride0 + __float2uint_rz(s1) * f.stride1 + __float2uint_rz(s2);
+  // Rounded down from q itself (floor(q) inside the grid), so that the cell
+  // index does not wait for the floor; the conversions saturate, and outside
+  // the grid the value is never used.
+  node = __float2uint_rd(q0) * f.stride0 + __float2uint_rd(q1) * f.stride1 + __float2uint_rd(q2);
   return inside;
 }
 
