@@ -256,6 +256,33 @@ __device__ __forceinline__ void gather(const FieldView& f, uint32_t node, Corner
   k.z37 = make_float2(z[3], z[7]);
 }
 
+// gather() of F32 nodes into CornerNodes only where `need` holds, by
+// predicated loads instead of a branch: elsewhere the corners keep their
+// values and no load is made.
+__device__ __forceinline__ void load_node_if(bool need, const float4* at, float& x, float& y,
+                                             float& z) {
+  float w = 0.0f;
+  asm("{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %5, 0;\n\t"
+      "@p ld.global.nc.v4.f32 {%0, %1, %2, %3}, [%4];\n\t}"
+      : "+f"(x), "+f"(y), "+f"(z), "+f"(w)
+      : "l"(at), "r"(need ? 1u : 0u));
+}
+
+__device__ __forceinline__ void gather_if(const FieldView& f, uint32_t node, bool need,
+                                          CornerNodes& k) {
+  const CellEdges<DPA_STORAGE_F32> c(f, node, 0);
+  float z[8] = {k.z04.x, k.z15.x, k.z26.x, k.z37.x, k.z04.y, k.z15.y, k.z26.y, k.z37.y};
+#pragma unroll
+  for (int e = 0; e < 4; ++e) {
+    load_node_if(need, c.e[e], k.xy[2 * e].x, k.xy[2 * e].y, z[2 * e]);
+    load_node_if(need, c.e[e] + 1, k.xy[2 * e + 1].x, k.xy[2 * e + 1].y, z[2 * e + 1]);
+  }
+  k.z04 = make_float2(z[0], z[4]);
+  k.z15 = make_float2(z[1], z[5]);
+  k.z26 = make_float2(z[2], z[6]);
+  k.z37 = make_float2(z[3], z[7]);
+}
+
 template <int kStorage>
 __device__ __forceinline__ void gather(const FieldView& f, uint32_t node, CornerEdges& k,
                                        int64_t slice_base = 0) {
@@ -364,7 +391,11 @@ struct CellSampler {
     uint32_t node;
     Weights w;
     const bool inside = locate<kLocate>(f, p, node, w);
-    if (inside && node != cached) {
+    const bool need = inside && node != cached;
+    if constexpr (kStorage == DPA_STORAGE_F32) {
+      gather_if(f, node, need, corners);
+      cached = need ? node : cached;
+    } else if (need) {
       gather<kStorage>(f, node, corners);
       cached = node;
     }
