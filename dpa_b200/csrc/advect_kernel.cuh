@@ -24,8 +24,8 @@ struct CurveCounter {
   uint32_t segments = 0;
   bool prev_open = false;  // previous kept vertex is not terminal-valued
 
-  __device__ __forceinline__ void append(float x, float y, float z) {
-    const bool valid = !equals3(x, y, z, kInvalid);
+  __device__ __forceinline__ void append(float x, float y, float z, bool taken = true) {
+    const bool valid = taken && !equals3(x, y, z, kInvalid);
     const bool terminal = equals3(x, y, z, kTerminal);
     segments += valid && !terminal && prev_open ? 1u : 0u;
     prev_open = valid ? !terminal : prev_open;
@@ -205,13 +205,15 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
         it[j] += taken ? 1u : 0u;
         if constexpr (kUnsteady) t[j] = taken ? __fadd_rn(t[j], a.coefficients.dt) : t[j];
         if constexpr (kRecord) {
-          if (taken) {
-            float* v = curve[j] + 3 * uint64_t(it[j]);
-            v[0] = p[j].p0;
-            v[1] = p[j].p21.y;
-            v[2] = p[j].p21.x;
-            counter[j].append(p[j].p0, p[j].p21.y, p[j].p21.x);
-          }
+          // The step's vertex, stored by predicated stores rather than a
+          // branch (a launch of few particles waits on each step's chain).
+          float* v = curve[j] + 3 * uint64_t(it[j]);
+          asm volatile(
+              "{\n\t.reg .pred p;\n\tsetp.ne.u32 p, %4, 0;\n\t"
+              "@p st.global.f32 [%0], %1;\n\t@p st.global.f32 [%0+4], %2;\n\t"
+              "@p st.global.f32 [%0+8], %3;\n\t}" ::"l"(v),
+              "f"(p[j].p0), "f"(p[j].p21.y), "f"(p[j].p21.x), "r"(taken ? 1u : 0u));
+          counter[j].append(p[j].p0, p[j].p21.y, p[j].p21.x, taken);
         }
         stop[j] = !taken || it[j] >= limit[j];
         halt = halt || (active[j] && stop[j]);
