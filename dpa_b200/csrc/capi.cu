@@ -578,8 +578,8 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
       storage != DPA_STORAGE_F32_EDGES)
     return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "unknown storage");
   for (int i = 0; i < 3; ++i) {
-    if (shape[i] == 0 || shape[i] > (1u << 24))
-      return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "field shape must be in [1, 2^24] per axis");
+    if (shape[i] == 0 || shape[i] > (1u << 23))
+      return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "field shape must be in [1, 2^23] per axis");
     if (!(spacing[i] > 0.0f) || !std::isfinite(spacing[i]) || !std::isfinite(offset[i]))
       return fail(ctx, DPA_ERROR_INVALID_ARGUMENT, "spacing must be positive and finite");
   }

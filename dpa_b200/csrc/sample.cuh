@@ -140,7 +140,16 @@ __device__ __forceinline__ bool locate(const FieldView& f, const Position& p, ui
   }
   const bool inside = (q0 >= 0.0f) && (q0 < f.upper[0]) && (q1 >= 0.0f) && (q1 < f.upper[1]) &&
                       (q2 >= 0.0f) && (q2 < f.upper[2]);
-  const float s0 = floorf(q0), s1 = floorf(q1), s2 = floorf(q2);
+  // floor(q) and its integer from one round-down add: for 0 <= q < 2^23,
+  // RD(q + 2^23) is 2^23 + floor(q), whose low mantissa bits are floor(q),
+  // and subtracting 2^23 again is exact. Inside the grid q < n - 1 <= 2^23
+  // (the field's axes hold at most 2^23 nodes); outside it neither value is
+  // used. (At q = -0 the floor is +0 instead of -0, which the weights' sign
+  // rules below undo.)
+  const float b0 = __fadd_rd(q0, 0x1p23f), b1 = __fadd_rd(q1, 0x1p23f),
+              b2 = __fadd_rd(q2, 0x1p23f);
+  const float s0 = __fsub_rn(b0, 0x1p23f), s1 = __fsub_rn(b1, 0x1p23f),
+              s2 = __fsub_rn(b2, 0x1p23f);
   if constexpr (kLocate == kLocatePow2) {
     w.w0 = copysignf(__fsub_rn(q0, s0), q0);
     const float2 d = sum2(make_float2(q2, q1), neg2(make_float2(s2, s1)));
@@ -160,10 +169,9 @@ __device__ __forceinline__ bool locate(const FieldView& f, const Position& p, ui
         weight_general<kLocate>(a21.x, s2, f.spacing[2], f.reciprocal[2], f.reciprocal_lo[2]),
         weight_general<kLocate>(a21.y, s1, f.spacing[1], f.reciprocal[1], f.reciprocal_lo[1]));
   }
-  // Rounded down from q itself (floor(q) inside the grid), so that the cell
-  // index does not wait for the floor; the conversions saturate, and outside
-  // the grid the value is never used.
-  node = __float2uint_rd(q0) * f.stride0 + __float2uint_rd(q1) * f.stride1 + __float2uint_rd(q2);
+  constexpr uint32_t kTwo23 = 0x4B000000u;  // the bits of 2^23
+  node = (__float_as_uint(b0) - kTwo23) * f.stride0 + (__float_as_uint(b1) - kTwo23) * f.stride1 +
+         (__float_as_uint(b2) - kTwo23);
   return inside;
 }
 
