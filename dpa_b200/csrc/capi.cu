@@ -636,9 +636,11 @@ static int create_field(dpa_context* ctx, const float* xyzv, bool device_input,
       v.reciprocal_lo[i] = lo;
       v.scaled_offset[i] = offset[i] * v.reciprocal[i];
       v.upper[i] = float(int64_t(shape[i]) - 1);
+      v.cells[i] = uint32_t(shape[i] - 1);
     }
     v.stride0 = uint32_t(shape[1] * shape[2]);
     v.stride1 = uint32_t(shape[2]);
+    v.node_bias = 0x4B000000u * (v.stride0 + v.stride1 + 1u);
     v.storage = storage;
     v.locate = dpa::kLocatePow2;
     if (!pow2 && ctx->ieee_division) {

@@ -49,6 +49,10 @@ struct FieldView {
   float reciprocal_lo[3];  // RN(1 / spacing - reciprocal)
   float scaled_offset[3];  // offset / spacing, exact; used by kLocatePow2 only
   float upper[3];          // n - 1: inside iff 0 <= (p - offset) / h < n - 1
+  uint32_t cells[3];       // n - 1, the cells per axis
+  // (2^23 as float bits) * (stride0 + stride1 + 1), modulo 2^32: what the
+  // cell index subtracts when it is formed from biased floors (sample.cuh).
+  uint32_t node_bias;
   int32_t storage;         // dpa_storage
   // LocateMode of the spatial axes. kLocatePow2 needs every spacing a power
   // of two in [2^-20, 2^20] and every offset zero or at least 2^-100 in

@@ -138,8 +138,6 @@ __device__ __forceinline__ bool locate(const FieldView& f, const Position& p, ui
       q1 = divide_spacing<kLocate>(a21.y, f.spacing[1], f.reciprocal[1], f.reciprocal_lo[1]);
     }
   }
-  const bool inside = (q0 >= 0.0f) && (q0 < f.upper[0]) && (q1 >= 0.0f) && (q1 < f.upper[1]) &&
-                      (q2 >= 0.0f) && (q2 < f.upper[2]);
   // floor(q) and its integer from one round-down add: for 0 <= q < 2^23,
   // RD(q + 2^23) is 2^23 + floor(q), whose low mantissa bits are floor(q),
   // and subtracting 2^23 again is exact. Inside the grid q < n - 1 <= 2^23
@@ -169,9 +167,15 @@ __device__ __forceinline__ bool locate(const FieldView& f, const Position& p, ui
         weight_general<kLocate>(a21.x, s2, f.spacing[2], f.reciprocal[2], f.reciprocal_lo[2]),
         weight_general<kLocate>(a21.y, s1, f.spacing[1], f.reciprocal[1], f.reciprocal_lo[1]));
   }
+  // The integer floors (the bits of b minus those of 2^23) decide inside:
+  // 0 <= q < n - 1 iff 0 <= floor(q) < n - 1, and a negative, NaN, infinite
+  // or too large q gives a difference of n - 1 or more as an unsigned value
+  // (-0 gives 0, inside, as the reference has it).
   constexpr uint32_t kTwo23 = 0x4B000000u;  // the bits of 2^23
-  node = (__float_as_uint(b0) - kTwo23) * f.stride0 + (__float_as_uint(b1) - kTwo23) * f.stride1 +
-         (__float_as_uint(b2) - kTwo23);
+  const uint32_t i0 = __float_as_uint(b0), i1 = __float_as_uint(b1), i2 = __float_as_uint(b2);
+  const bool inside =
+      (i0 - kTwo23 < f.cells[0]) & (i1 - kTwo23 < f.cells[1]) & (i2 - kTwo23 < f.cells[2]);
+  node = i0 * f.stride0 + i1 * f.stride1 + i2 - f.node_bias;
   return inside;
 }
 

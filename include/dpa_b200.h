@@ -202,7 +202,9 @@ int dpa_integrator_from_name(const char* name, int32_t* integrator);
 
 /* Replaces regular_grid_loader::load_vector_field (regular_grid_loader.cpp:65-88):
  * uploads a host XYZV field and repacks it for the device in the given storage.
- * offset/spacing are the grid's world offset and cell spacing. */
+ * offset/spacing are the grid's world offset and cell spacing. Each axis holds
+ * 1 to 2^23 nodes, and a slice fewer than 2^32 (DPA_ERROR_INVALID_ARGUMENT
+ * otherwise). */
 int dpa_field_create(dpa_context* ctx, const float* xyzv, const uint64_t shape[3],
                      const float offset[3], const float spacing[3], int32_t storage,
                      dpa_field** out);
