@@ -78,7 +78,14 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
   if (lane == 0) warp_claim[0] = warp_claim[1] = 0;
   __syncwarp();
   bool exhausted = false;
-  const float nan = __int_as_float(0x7fffffff);
+  // Where an empty slot waits: the centre of the first cell, so that a step
+  // run for it (branch-free steppers) divides normal numbers and loads its
+  // corners once.
+  const Position parked{__fmaf_rn(0.5f, f.spacing[0], f.offset[0]),
+                        make_float2(__fmaf_rn(0.5f, f.spacing[2], f.offset[2]),
+                                    __fmaf_rn(0.5f, f.spacing[1], f.offset[1]))};
+  constexpr bool kStepAll = !kUnsteady && (kIntegrator == DPA_INTEGRATOR_EULER ||
+                                           kIntegrator == DPA_INTEGRATOR_RUNGE_KUTTA_4);
 
   bool active[kPPT];
   Position p[kPPT];
@@ -90,7 +97,7 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
 #pragma unroll
   for (int j = 0; j < kPPT; ++j) {
     active[j] = false;
-    p[j] = Position{nan, make_float2(nan, nan)};
+    p[j] = parked;
     history[j] = StepHistory{};
     t[j] = 0.0f;
     curve[j] = nullptr;
@@ -192,12 +199,18 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
       halt = halt || stop[j];
     }
     while (!__any_sync(kFull, halt)) {
-      // An empty slot does not step: its NaN position would send IEEE
-      // division into its slow path, which the whole warp would wait for.
+      // Branch-free steppers run every slot, an empty one without moving it;
+      // the others skip empty slots.
 #pragma unroll
-      for (int j = 0; j < kPPT; ++j)
-        r[j] = active[j] ? step<kIntegrator>(f, a.coefficients, sampler[j], p[j], t[j], history[j])
-                         : int(kStepOutOfBounds);
+      for (int j = 0; j < kPPT; ++j) {
+        if constexpr (kStepAll)
+          r[j] = step<kIntegrator>(f, a.coefficients, sampler[j], p[j], t[j], history[j],
+                                   active[j]);
+        else
+          r[j] = active[j]
+                     ? step<kIntegrator>(f, a.coefficients, sampler[j], p[j], t[j], history[j])
+                     : int(kStepOutOfBounds);
+      }
       halt = false;
 #pragma unroll
       for (int j = 0; j < kPPT; ++j) {
@@ -265,7 +278,7 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
       if (a.in_flight && reason != DPA_TERMINATION_IN_FLIGHT)
         atomicSub(a.in_flight + a.request_of[k], 1u);
       active[j] = false;
-      p[j] = Position{nan, make_float2(nan, nan)};
+      p[j] = parked;
     }
   }
 }

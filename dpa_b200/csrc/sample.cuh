@@ -562,10 +562,12 @@ __device__ __forceinline__ void general_step(const GeneralCoefficients& g, float
 // (p2, p1) is (v0, v1) (particle_advector.cpp:369).
 // t is the particle's time (used by time-varying fields only); the caller
 // advances it by dt after a step is taken.
+// active: false for an empty slot, which the branch-free steps below run
+// through without moving it (its position is parked inside the grid).
 template <int kIntegrator, class Sampler>
 __device__ __forceinline__ int step(const FieldView& f, const StepCoefficients& k,
                                    Sampler& sampler, Position& p, float t,
-                                   StepHistory& history) {
+                                   StepHistory& history, bool active = true) {
   float2 v01;
   float v2;
   if constexpr (Sampler::kSteady && (kIntegrator == DPA_INTEGRATOR_EULER ||
@@ -586,10 +588,12 @@ __device__ __forceinline__ int step(const FieldView& f, const StepCoefficients& 
       const float2 n0 = mul2(splat(k.c0), v01), n1 = mul2(splat(k.c1), v01);
       n.p21 = add2(add2(add2(add2(p.p21, n0), n1), n1), n0);
     }
-    const bool taken = inside && !zero;
+    const bool taken = active && inside && !zero;
     p.p0 = taken ? n.p0 : p.p0;
     p.p21 = make_float2(taken ? n.p21.x : p.p21.x, taken ? n.p21.y : p.p21.y);
-    return !inside ? int(kStepOutOfBounds) : zero ? int(kStepZeroVelocity) : int(kStepTaken);
+    return !(active && inside) ? int(kStepOutOfBounds)
+           : zero              ? int(kStepZeroVelocity)
+                               : int(kStepTaken);
   }
   if (!sampler.sample(f, p, t, v01, v2)) return kStepOutOfBounds;
   if (is_zero(v01, v2)) return kStepZeroVelocity;
