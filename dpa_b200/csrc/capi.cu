@@ -1134,7 +1134,10 @@ int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_adve
         cudaEventElapsedTime(&ms, e0, e1);
         if (rep > 0 && (best_ms == 0.0f || ms < best_ms)) best_ms = ms;
       }
-      if (rc == DPA_OK && (first || best_ms < winner_ms)) {
+      // A later setting replaces the winner only if it is at least 3 %
+      // faster: timings of a sample vary by about that much, and the search
+      // tries the defaults first.
+      if (rc == DPA_OK && (first || best_ms < 0.97f * winner_ms)) {
         winner = ctx->tuning;
         winner_ms = best_ms;
         first = false;

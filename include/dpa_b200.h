@@ -333,9 +333,10 @@ int dpa_context_get_tuning(const dpa_context* ctx, dpa_tuning* tuning);
  * group at a time from the defaults, keeping the best so far: processing order
  * (64 / 16 / off), then launch shape (256, 128 or 64 threads per block, one or
  * two particles per lane), then claim size (16..128) with blocks per SM (all
- * that fit, 3, 2). The processing order pays off with particle density and run
- * length, so a sample as dense and as long as the real run picks the setting
- * that run wants. */
+ * that fit, 3, 2). A setting tried later replaces the best so far only when
+ * it is at least 3 % faster. The processing order pays off with particle
+ * density and run length, so a sample as dense and as long as the real run
+ * picks the setting that run wants. */
 int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_advect_options* options,
                         uint64_t count, const float* device_positions,
                         const uint64_t* device_remaining, uint64_t sample_steps,
