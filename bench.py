@@ -286,11 +286,26 @@ def within_horizon(err, bar=0.99):
     return best
 
 
+KERNEL_SOURCES = ["advect_kernel.cuh", "sample.cuh", "common.cuh", "kernels.cuh", "advect.cu",
+                  "advect_f32.cu", "advect_f32e.cu", "advect_f16.cu", "advect_bf16.cu"]
+
+
+def kernel_sources_digest():
+    """SHA-256 of the sources that make up the advection kernels (the
+    figures of a capture depend on these alone)."""
+    import hashlib
+    h = hashlib.sha256()
+    for name in KERNEL_SOURCES:
+        h.update(name.encode())
+        h.update((ROOT / "dpa_b200" / "csrc" / name).read_bytes())
+    return h.hexdigest()
+
+
 def traffic_profile(key):
     """Per-particle-step figures of one workload's advection kernel from the
     committed ncu capture (profiles/advect_traffic.json): DRAM bytes, L1TEX
-    bytes and issue activity, with the digest of the sources they were
-    captured from and whether the library built here has the same sources."""
+    bytes and issue activity, with the digest of the kernel sources they were
+    captured from and whether the sources here are the same."""
     try:
         d = json.loads(TRAFFIC_FILE.read_text())
     except Exception:
@@ -299,10 +314,9 @@ def traffic_profile(key):
     if not entry:
         return None
     entry = dict(entry)
-    stamp = ROOT / "dpa_b200" / "libdpa_b200.so.stamp"
     try:
         entry["captured_with_current_sources"] = \
-            stamp.read_text().strip() == d.get("sources_digest")
+            kernel_sources_digest() == d.get("kernel_sources_digest")
     except Exception:
         entry["captured_with_current_sources"] = None
     return entry

@@ -1145,7 +1145,10 @@ int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_adve
     };
     // Coordinate search from the defaults: processing order, then the launch
     // shape (threads per block and particles per lane), then claim size and
-    // blocks per SM, each step keeping the best setting so far.
+    // blocks per SM, each step keeping the best setting so far. Claims stay
+    // small: a warp that claimed many entries works through them one lifetime
+    // after another once the order runs out, which a sample with a step cap
+    // does not show.
     for (uint32_t order : {64u, 16u, 0u}) {
       if (rc != DPA_OK) break;
       ctx->tuning = dpa_tuning_state{};
@@ -1163,7 +1166,7 @@ int dpa_autotune_advect(dpa_context* ctx, const dpa_field* field, const dpa_adve
       }
     const dpa_tuning_state after_shape = winner;
     for (uint32_t grid : {0u, 3u, 2u})
-      for (uint32_t claim : {16u, 32u, 64u, 128u}) {
+      for (uint32_t claim : {16u, 32u}) {
         if (rc != DPA_OK) break;
         ctx->tuning = after_shape;
         ctx->tuning.blocks_per_sm = grid;

@@ -332,7 +332,7 @@ int dpa_context_get_tuning(const dpa_context* ctx, dpa_tuning* tuning);
  * the context and returns it in best (may be NULL). The search goes one knob
  * group at a time from the defaults, keeping the best so far: processing order
  * (64 / 16 / off), then launch shape (256, 128 or 64 threads per block, one or
- * two particles per lane), then claim size (16..128) with blocks per SM (all
+ * two particles per lane), then claim size (16 or 32) with blocks per SM (all
  * that fit, 3, 2). A setting tried later replaces the best so far only when
  * it is at least 3 % faster. The processing order pays off with particle
  * density and run length, so a sample as dense and as long as the real run
