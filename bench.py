@@ -851,6 +851,7 @@ def batched_config(ctx, stream, a, reps=2):
     from dpa_b200 import _native as N
     from dpa_b200 import fields, seeds
     lib = ctx._lib
+    ctx.check(lib.dpa_context_set_profiling(ctx.handle, 1))
     n_grid = a.batch_n
     grid = fields.curl_noise(n_grid, 8.0, 3, device="cuda")
     torch.cuda.empty_cache()
