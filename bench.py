@@ -290,14 +290,25 @@ KERNEL_SOURCES = ["advect_kernel.cuh", "sample.cuh", "common.cuh", "kernels.cuh"
                   "advect_f32.cu", "advect_f32e.cu", "advect_f16.cu", "advect_bf16.cu"]
 
 
+def _code_lines(text):
+    """The lines of a source with `//` comments, trailing blanks and empty
+    lines removed (the kernel sources hold no `//` inside string literals)."""
+    out = []
+    for line in text.splitlines():
+        code = line.split("//", 1)[0].rstrip()
+        if code:
+            out.append(code)
+    return "\n".join(out)
+
+
 def kernel_sources_digest():
-    """SHA-256 of the sources that make up the advection kernels (the
-    figures of a capture depend on these alone)."""
+    """SHA-256 of the code of the sources that make up the advection kernels
+    (the figures of a capture depend on these alone; comments do not count)."""
     import hashlib
     h = hashlib.sha256()
     for name in KERNEL_SOURCES:
         h.update(name.encode())
-        h.update((ROOT / "dpa_b200" / "csrc" / name).read_bytes())
+        h.update(_code_lines((ROOT / "dpa_b200" / "csrc" / name).read_text()).encode())
     return h.hexdigest()
 
 

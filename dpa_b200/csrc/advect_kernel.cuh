@@ -54,8 +54,11 @@ constexpr int advect_min_blocks() {
 // the warp's particles stops, with one vote per step and a 32-bit step
 // counter per stretch (a stretch ends at 2^32 - 1 steps at the latest). The
 // kPPT slots of a lane step in lock-step, so one particle's corner gather is
-// in flight while the other's arithmetic issues. An empty slot holds a NaN
-// position and takes no steps.
+// in flight while the other's arithmetic issues. An empty slot holds a parked
+// position, the centre of the first cell (never NaN, which would send the
+// division of a step into its slow path for the whole warp). With one
+// particle per lane the branch-free steady Euler and RK4 steppers step a
+// parked slot and discard the result; otherwise an empty slot takes no steps.
 template <int kIntegrator, int kStorage, int kLocate, bool kRecord, bool kUnsteady, int kPPT>
 __global__ void __launch_bounds__(kAdvectBlock, advect_min_blocks<kIntegrator, kUnsteady, kPPT>())
 advect_kernel(const FieldView f, const AdvectArgs a) {
