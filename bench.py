@@ -1106,7 +1106,11 @@ def serving_run(a, ctx, arrival_seed=4, storage="f16", probe=False):
            "by_kind": by_kind,
            "particle_steps_per_s": steps / wall, "ticks": int(stats["ticks"]),
            "launches": int(stats["launches"]), "busy_seconds": float(stats["busy_seconds"]),
-           "tick_device_seconds": float(stats["tick_device_seconds"]), "mix": kinds}
+           "tick_device_seconds": float(stats["tick_device_seconds"]),
+           "admission": {k: stats[k] for k in ("peak_slots", "peak_vertices", "slot_refusals",
+                                                "vertex_refusals", "overdue_scans",
+                                                "peak_finishing", "finish_seconds")},
+           "mix": kinds}
     if probe and probes:
         ob = _oracle()
         og = ob.OracleGrid.of(grid)

@@ -149,6 +149,14 @@ class ServerStats(C.Structure):
         ("queued", C.c_uint32),
         ("active", C.c_uint32),
         ("tick_device_seconds", C.c_double),
+        ("peak_slots", C.c_uint64),
+        ("peak_vertices", C.c_uint64),
+        ("slot_refusals", C.c_uint64),
+        ("vertex_refusals", C.c_uint64),
+        ("overdue_scans", C.c_uint64),
+        ("peak_finishing", C.c_uint32),
+        ("reserved0", C.c_uint32),
+        ("finish_seconds", C.c_double),
     ]
 
 

@@ -113,6 +113,7 @@ struct dpa_server {
   std::deque<pending> queue;
   std::vector<active_request> active;
   uint64_t used_slots = 0;
+  uint64_t used_vertices = 0;
   dpa::admission_config admission;
   std::map<uint64_t, int32_t> drop_requests;  // id -> status, from dpa_server_cancel
   std::map<uint64_t, std::unique_ptr<response_storage>> done, handed_out;
@@ -220,9 +221,13 @@ void dpa_server::select(std::vector<active_request>& out) {
       [&](const pending& p) {
         const dpa_request& q = p.request;
         const uint64_t raw_need = q.record ? q.count * (q.iterations + 2) : 0;
-        if (!slots.allocate(q.count, &first)) return false;
+        if (!slots.allocate(q.count, &first)) {
+          ++stats.slot_refusals;
+          return false;
+        }
         if (!vertices.allocate(raw_need, &raw_first)) {
           slots.release(first, q.count);
+          ++stats.vertex_refusals;
           return false;
         }
         return true;
@@ -236,9 +241,14 @@ void dpa_server::select(std::vector<active_request>& out) {
         a.first = first;
         a.raw_first = raw_first;
         a.admitted = t;
+        used_vertices += a.raw_count;
         out.push_back(std::move(a));
       },
       [&] { return !free_counters.empty(); });
+  stats.peak_slots = std::max(stats.peak_slots, used_slots);
+  stats.peak_vertices = std::max(stats.peak_vertices, used_vertices);
+  if (!queue.empty() && t - queue.front().queued >= admission.max_bypass_seconds)
+    ++stats.overdue_scans;
 }
 
 // Called with the mutex held: returns the waiting requests that have passed
@@ -651,6 +661,7 @@ void dpa_server::run() {
           active.erase(active.begin() + long(i));
           handed = true;
         }
+        stats.peak_finishing = std::max(stats.peak_finishing, uint32_t(finishing.size()));
         if (handed) finish_wake.notify_one();
         pending = false;
       }
@@ -685,11 +696,14 @@ void dpa_server::run_finisher() {
         finishing.pop_front();
       }
       auto out = std::make_unique<response_storage>();
+      const auto f0 = clock_type::now();
       finish(a, *out);
       std::lock_guard<std::mutex> lock(mutex);
+      stats.finish_seconds += std::chrono::duration<double>(clock_type::now() - f0).count();
       slots.release(a.first, a.p.request.count);
       used_slots -= a.p.request.count;
       vertices.release(a.raw_first, a.raw_count);
+      used_vertices -= a.raw_count;
       free_counters.push_back(a.slot);
       stats.particle_steps += out->r.particle_steps;
       stats.completed += 1;

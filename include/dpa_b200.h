@@ -446,6 +446,17 @@ typedef struct dpa_server_stats {
   double   tick_device_seconds;  /* device time of the ticks (their launches, in
                                     stream order; overlapping finishing work on
                                     the finisher's stream is not counted) */
+  /* Where admission waited (for tuning arena sizes and admission options): */
+  uint64_t peak_slots;           /* most particle slots in use at once */
+  uint64_t peak_vertices;        /* most curve-staging vertices in use at once */
+  uint64_t slot_refusals;        /* admission attempts the slot arena had no room for */
+  uint64_t vertex_refusals;      /* ... the curve-staging arena had no room for */
+  uint64_t overdue_scans;        /* admission scans that ended with the oldest request
+                                    past max_bypass_ms still waiting (nothing
+                                    younger passed it) */
+  uint32_t peak_finishing;       /* most finished requests waiting for the finisher */
+  uint32_t reserved0;
+  double   finish_seconds;       /* finisher time spent returning requests */
 } dpa_server_stats;
 
 int dpa_server_create(dpa_context* ctx, const dpa_server_options* options, dpa_server** out);

@@ -66,3 +66,42 @@ def test_device_count_and_context_without_gpu():
     assert n.value == 0
     with pytest.raises(dpa_b200.DpaError):
         dpa_b200.Context(0)
+
+
+# ctypes mirrors of the header's structures, by typedef name.
+STRUCTS = {
+    "dpa_advect_options": N.AdvectOptions,
+    "dpa_curve_chunk": N.CurveChunk,
+    "dpa_tuning": N.Tuning,
+    "dpa_server_options": N.ServerOptions,
+    "dpa_request": N.Request,
+    "dpa_response": N.Response,
+    "dpa_server_stats": N.ServerStats,
+}
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """Every ctypes structure has the size and field offsets that a C compiler
+    gives the header's typedef (a field added on one side only would shift
+    the fields after it)."""
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "dpa_b200.h"',
+             "int main(void) {"]
+    for cname, py in STRUCTS.items():
+        lines.append(f'  printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", str(HEADER.parent), str(src), "-o", str(exe)],
+                   check=True, capture_output=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                               text=True).stdout.splitlines():
+        cname, what, value = line.split()
+        got[(cname, what)] = int(value)
+    for cname, py in STRUCTS.items():
+        assert got[(cname, "sizeof")] == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)

@@ -68,6 +68,9 @@ def test_results_are_the_same_alone_and_in_the_mix(ctx, resident):
             results[res.id] = res
         stats = server.stats()
     assert stats["completed"] == len(reqs) and stats["ticks"] > 1
+    # Where admission and the finishers spent their time.
+    assert 0 < stats["peak_slots"] <= 40000 and stats["peak_vertices"] <= 4_000_000
+    assert stats["peak_finishing"] >= 1 and stats["finish_seconds"] > 0
     for rid, r in ids.items():
         res = results[rid]
         assert res.status == 0
