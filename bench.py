@@ -984,8 +984,9 @@ def serving_run(a, ctx, arrival_seed=4, storage="f16", probe=False):
     link carries, so their queue would grow without bound; at 2e4 seeds the
     curves need about a quarter of the link. Iterations uniform in [100,
     5000]. Admission passes small requests (at most 65,536 seeds) past large
-    ones that wait for room, keeps 10 % of the slots for them and lets the
-    oldest request be passed for at most 250 ms. Latency is submit to result;
+    ones that wait for room, keeps 10 % of the 12 M slots for them and lets
+    the oldest request be passed by large ones for at most 250 ms (small ones
+    keep passing it within that 10 %). Latency is submit to result;
     throughput counts particle-steps over the wall time of the run. Results
     are returned in an 8 GiB pinned arena and dropped once their times are
     read (no copy), except (probe) for a few

@@ -113,6 +113,7 @@ struct dpa_server {
   std::deque<pending> queue;
   std::vector<active_request> active;
   uint64_t used_slots = 0;
+  uint64_t small_slots = 0;  // of used_slots, held by small requests
   uint64_t used_vertices = 0;
   dpa::admission_config admission;
   std::map<uint64_t, int32_t> drop_requests;  // id -> status, from dpa_server_cancel
@@ -216,7 +217,7 @@ void dpa_server::select(std::vector<active_request>& out) {
   const double t = now();
   uint64_t first = 0, raw_first = 0;
   dpa::admit_waiting(
-      queue, admission, used_slots, [](const pending& p) { return p.request.count; },
+      queue, admission, used_slots, small_slots, [](const pending& p) { return p.request.count; },
       [&](const pending& p) { return t - p.queued; },
       [&](const pending& p) {
         const dpa_request& q = p.request;
@@ -702,6 +703,7 @@ void dpa_server::run_finisher() {
       stats.finish_seconds += std::chrono::duration<double>(clock_type::now() - f0).count();
       slots.release(a.first, a.p.request.count);
       used_slots -= a.p.request.count;
+      if (a.p.request.count <= admission.small_seeds) small_slots -= a.p.request.count;
       vertices.release(a.raw_first, a.raw_count);
       used_vertices -= a.raw_count;
       free_counters.push_back(a.slot);

@@ -383,7 +383,9 @@ typedef struct dpa_server_options {
                                   reserved slots (0: 65536) */
   uint32_t reserved_percent;   /* share of the slots kept for small requests (0-90) */
   uint32_t max_bypass_ms;      /* how long the oldest waiting request may be passed
-                                  by younger ones that fit (0: 250 ms) */
+                                  by younger ones that fit (0: 250 ms); after that
+                                  no large request passes it, and small ones only
+                                  within the reserved share */
   uint64_t response_bytes;     /* pinned host memory for returned arrays (0: 256 MiB);
                                   a response that does not fit it is returned from
                                   pageable memory */
@@ -452,8 +454,8 @@ typedef struct dpa_server_stats {
   uint64_t slot_refusals;        /* admission attempts the slot arena had no room for */
   uint64_t vertex_refusals;      /* ... the curve-staging arena had no room for */
   uint64_t overdue_scans;        /* admission scans that ended with the oldest request
-                                    past max_bypass_ms still waiting (nothing
-                                    younger passed it) */
+                                    past max_bypass_ms still waiting (no large
+                                    request passed it) */
   uint32_t peak_finishing;       /* most finished requests waiting for the finisher */
   uint32_t reserved0;
   double   finish_seconds;       /* finisher time spent returning requests */

@@ -265,3 +265,40 @@ def test_small_requests_pass_a_large_one_that_waits_for_room(ctx, resident):
         assert_same(results[rid].positions, want.inactive_particles.position)
     want = alone(ctx, field, big, 300, "runge_kutta_4", 0.01, False)
     assert_same(results[second].positions, want.inactive_particles.position)
+
+
+def test_an_overdue_request_holds_large_ones_and_lets_small_ones_pass(ctx, resident):
+    """Once the oldest waiting request is past max_bypass_ms, a younger large
+    request that would fit waits behind it, while small requests still pass
+    within the reserved share; results are the same as alone."""
+    grid, field = resident["noise"]
+    offset, size = seeds.seed_box(grid)
+    box = ([0.0] * 3, [float(s - 1) for s in grid.shape])
+    big = seeds.generate_random(offset, size, 12000, 0, aabb=box, seed=81).position
+    mid = seeds.generate_random(offset, size, 1500, 0, aabb=box, seed=82).position
+    small = [seeds.generate_random(offset, size, 200, 0, aabb=box, seed=90 + i).position
+             for i in range(3)]
+    with Server(ctx, particle_capacity=20000, vertex_capacity=0, steps_per_tick=8,
+                max_requests=16, small_request_seeds=1000, reserved_percent=10,
+                max_bypass_ms=1) as server:
+        fid = server.add_field(field)
+        first = server.submit(fid, big, 30000, step_size=0.01)  # runs
+        second = server.submit(fid, big, 300, step_size=0.01)   # no room: waits, overdue
+        time.sleep(0.01)
+        third = server.submit(fid, mid, 200)                    # fits, but is large
+        smalls = [server.submit(fid, s, 100) for s in small]    # pass it
+        results = {}
+        while len(results) < 3 + len(smalls):
+            res = server.poll(wait_ms=10000)
+            assert res is not None, server.stats()
+            results[res.id] = res
+        stats = server.stats()
+    assert all(r.status == 0 for r in results.values())
+    assert stats["overdue_scans"] > 0
+    assert all(results[s].admitted < results[second].admitted for s in smalls)
+    assert results[third].admitted >= results[second].admitted
+    for rid, s in zip(smalls, small):
+        want = alone(ctx, field, s, 100, "runge_kutta_4", 0.25, False)
+        assert_same(results[rid].positions, want.inactive_particles.position)
+    want = alone(ctx, field, mid, 200, "runge_kutta_4", 0.25, False)
+    assert_same(results[third].positions, want.inactive_particles.position)

@@ -118,13 +118,14 @@ struct req { int id; uint64_t seeds; double queued; };
 // Runs one admission scan at time `now` over `q` with `free_slots` free (of
 // `capacity`, allocated first fit) and returns the admitted ids in order.
 static std::vector<int> scan(std::deque<req>& q, const dpa::admission_config& c, uint64_t used,
-                             double now, int counters = 1000) {
+                             double now, int counters = 1000, uint64_t small = 0) {
   dpa::range_allocator slots(c.slot_capacity);
   uint64_t at = 0;
   if (used) slots.allocate(used, &at);
   std::vector<int> got;
   dpa::admit_waiting(
-      q, c, used, [](const req& r) { return r.seeds; }, [&](const req& r) { return now - r.queued; },
+      q, c, used, small, [](const req& r) { return r.seeds; },
+      [&](const req& r) { return now - r.queued; },
       [&](const req& r) { uint64_t o; return slots.allocate(r.seeds, &o); },
       [&](req& r) { got.push_back(r.id); --counters; }, [&] { return counters > 0; });
   return got;
@@ -154,10 +155,22 @@ int main() {
     const auto got2 = scan(q2, c, 880, 0.5);
     if (got2 != std::vector<int>({7})) return fail("a large request took reserved slots");
   }
-  {  // Once the oldest has waited max_bypass_seconds, nothing passes it...
-    std::deque<req> q = {{1, 600, 0.0}, {2, 5, 0.1}};
-    const auto got = scan(q, c, 500, 1.5);
-    if (!got.empty() || q.size() != 2) return fail("a request passed the overdue head");
+  {  // Once the oldest has waited max_bypass_seconds, no large request passes
+     // it; small ones still do, while all small requests stay in the reserve...
+    std::deque<req> q = {{1, 600, 0.0}, {2, 5, 0.1}, {3, 50, 0.2}, {4, 8, 0.3}};
+    const auto got = scan(q, c, 500, 1.5, 1000, 0);  // the head has no room
+    if (got != std::vector<int>({2, 4}) || q.size() != 2 || q.front().id != 1 ||
+        q.back().id != 3)
+      return fail("an overdue head: large requests passed it or small ones did not");
+    std::deque<req> q2 = {{1, 600, 0.0}, {2, 5, 0.1}, {3, 8, 0.2}};
+    const auto got2 = scan(q2, c, 500, 1.5, 1000, 90);  // 90 of 100 reserved slots held
+    if (got2 != std::vector<int>({2}) || q2.size() != 2)
+      return fail("small requests passed an overdue head beyond the reserve");
+    c.reserved_slots = 0;  // no reserve: nothing passes an overdue head
+    std::deque<req> q3 = {{1, 600, 0.0}, {2, 5, 0.1}};
+    const auto got3 = scan(q3, c, 500, 1.5);
+    c.reserved_slots = 100;
+    if (!got3.empty() || q3.size() != 2) return fail("a request passed the overdue head");
   }
   {  // ...and it may then take reserved slots.
     std::deque<req> q = {{1, 950, 0.0}, {2, 5, 0.1}};
