@@ -1101,6 +1101,7 @@ def serving_run(a, ctx, arrival_seed=4, storage="f16", probe=False):
     out = {"arrival_seed": arrival_seed, "requests": len(plan), "completed": len(results),
            "failed": sum(1 for r in results if r.status != 0),
            "wall_seconds": wall,
+           "_latencies_ms": lat,  # pooled over the runs by serving_config, then dropped
            "latency_ms": {"p50": float(np.percentile(lat, 50)),
                           "p99": float(np.percentile(lat, 99)), "max": float(lat.max())},
            "queue_wait_ms": pct([r.admitted - r.queued for r in results]),
@@ -1137,11 +1138,17 @@ def serving_config(a, ctx):
     runs = [serving_run(a, ctx, arrival_seed=4 + i, probe=(i == 0)) for i in range(a.serve_runs)]
     p99 = [r["latency_ms"]["p99"] for r in runs]
     p50 = [r["latency_ms"]["p50"] for r in runs]
+    # One 20 s run holds ~4,000 requests, so its p99 rests on its ~40 slowest;
+    # the pooled figures take every request of every run.
+    pooled = np.concatenate([r.pop("_latencies_ms") for r in runs])
     return {"rate_per_s": 200.0, "seconds_of_arrivals_per_run": a.serve_seconds,
             "field_storage": "f16", "runs": runs,
             "latency_ms": {"p50_median": statistics.median(p50), "p99_median": statistics.median(p99),
                            "p99_min": min(p99), "p99_max": max(p99),
-                           "p99_spread": max(p99) / max(min(p99), 1e-9)},
+                           "p99_spread": max(p99) / max(min(p99), 1e-9),
+                           "p50_pooled": float(np.percentile(pooled, 50)),
+                           "p99_pooled": float(np.percentile(pooled, 99)),
+                           "requests_pooled": int(pooled.size)},
             "particle_steps_per_s": statistics.mean(r["particle_steps_per_s"] for r in runs),
             "fp64_error_served": runs[0].get("fp64_error_served")}
 
